@@ -1,0 +1,360 @@
+"""Throughput benchmark of the time-based power walk on one or more B200s.
+
+Workload: the flat synthetic sky130hd design (200k cells, 10k cycles of
+2 ns at 1 ps ticks, per-net toggle probability U[0.05, 0.3], glitch pulses
+p=0.05 of 5-100 ps); ~4e8 net events. One step = one full evaluation of the
+trace: clear accumulators, walk every cell over every cycle, finalize the
+per-cell and per-cycle outputs.
+
+  value : net events / s with the event CSR resident in HBM
+  e2e   : the same through the public host API (B200Power.read_power_activities
+          from pinned host memory + fetch of per-cell/per-cycle results)
+
+Multi-GPU (torchrun, --gpus N): every rank evaluates its own trace of the same
+design (independent seeds); no collective is needed (weak scaling).
+--impl reference times the CPU restatement of the reference CPU path (FP32,
+static thread split as power/Power.cc:227-386) on the host cores over a
+bounded sample of cells.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "net events/s (time-based power walk, flat synthetic 200k cells x 10k cycles)"
+UNIT = "events/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=200_000)
+    ap.add_argument("--cycles", type=int, default=10_000)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cycles-per-tile", type=int, default=0)
+    ap.add_argument("--gates-per-block", type=int, default=0)
+    ap.add_argument("--threads-per-block", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(args, rank: int):
+    from gtpower_b200 import synth
+    spec = synth.FlatSpec(n_cell=args.cells, n_cycle=args.cycles, seed=20261203 + 1)
+    design, info = synth.flat_design(spec)
+    trace = synth.Trace(design, info, synth.TraceSpec(), seed=20261203 + 1 + 1000 * rank)
+    return design, info, trace
+
+
+def algorithmic_bytes(design, n_event: int) -> int:
+    """8 B tick + 2 bits per net event, CSR offsets, 24 B of attributes per
+    pin, the LUT floats, and 20 B of outputs per cell and per cycle."""
+    return int(8 * n_event + (n_event + 3) // 4 + 8 * (design.n_net + 1) + 24 * design.n_pin
+               + 4 * int(design.lib.lut_pool.shape[0]) + 20 * design.n_cell + 20 * design.n_period)
+
+
+def pin_events(design, net_off: np.ndarray) -> int:
+    cnt = np.diff(net_off)
+    p = design.pin_net
+    return int(cnt[p[p >= 0]].sum())
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self) -> dict:
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=6)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(design, ev, sample_seconds: float, total_events: int, total_pin_events: int):
+    """FP32 restatement of the reference CPU path on a bounded cell sample,
+    all host threads; extrapolated to net events/s of the whole trace."""
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    order = rng.permutation(design.n_cell).astype(np.int32)
+    cnt = np.diff(ev.net_off)
+    cell_pin_ev = np.add.reduceat(
+        np.where(design.pin_net >= 0, cnt[np.maximum(design.pin_net, 0)], 0), design.cell_pin_off[:-1])
+    # calibrate on a small slice, then size the sample to ~sample_seconds
+    k0 = max(threads * 4, 200)
+    r0 = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
+    pe0 = int(cell_pin_ev[order[:k0]].sum())
+    rate = pe0 / max(r0.seconds, 1e-6)
+    k = int(min(design.n_cell, max(k0, k0 * sample_seconds / max(r0.seconds, 1e-6))))
+    r = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k], outputs=False)
+    pe = int(cell_pin_ev[order[:k]].sum())
+    frac = pe / max(total_pin_events, 1)
+    ev_per_s = total_events * frac / max(r.seconds, 1e-9)
+    return {"value": ev_per_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"{k} of {design.n_cell} cells (random), {pe} of {total_pin_events} pin events, "
+                       f"{r.seconds:.2f} s on {threads} threads; extrapolated by pin-event share"),
+            "seconds": r.seconds}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    design, info, trace = workload(args, 0)
+    ev = trace.full()
+    total_events = ev.n_event
+    tpe = pin_events(design, ev.net_off)
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(11)
+    order = rng.permutation(design.n_cell).astype(np.int32)
+    cnt = np.diff(ev.net_off)
+    cell_pin_ev = np.add.reduceat(
+        np.where(design.pin_net >= 0, cnt[np.maximum(design.pin_net, 0)], 0), design.cell_pin_off[:-1])
+    # size each step's sample to ~10 s of host work
+    k0 = max(threads * 4, 200)
+    r0 = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
+    k = int(min(design.n_cell, max(k0, k0 * 10.0 / max(r0.seconds, 1e-6))))
+    for w in range(args.warmup):
+        orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
+    secs = []
+    pes = []
+    for s in range(args.steps):
+        sel = np.roll(order, -s * k)[:k]
+        r = orc.run(design, ev, fp32=True, threads=threads, cells=sel, outputs=False)
+        secs.append(r.seconds)
+        pes.append(int(cell_pin_ev[sel].sum()))
+    # whole-job time = sample time scaled by pin-event share
+    job_s = [t * tpe / max(pe, 1) for t, pe in zip(secs, pes)]
+    ms = float(np.mean(job_s)) * 1e3
+    value = total_events / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"flat synthetic sky130hd {args.cells} cells x {args.cycles} cycles",
+                       "n_event": total_events, "pin_events": tpe},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{k} random cells per step ({np.mean(pes):.3g} pin events), "
+                                       f"extrapolated by pin-event share"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    from gtpower_b200 import B200Power
+    from gtpower_b200.design import Events
+
+    design, info, trace = workload(args, rank)
+    t0 = time.time()
+    ev = trace.full()
+    gen_s = time.time() - t0
+    n_event = ev.n_event
+    tpe = pin_events(design, ev.net_off)
+
+    # pinned host copies (e2e leg) and device copies (value leg)
+    h_off = torch.from_numpy(ev.net_off).pin_memory()
+    h_t = torch.from_numpy(ev.time).pin_memory()
+    h_v = torch.from_numpy(ev.packed.view(np.int32)).pin_memory()
+    pinned = Events(h_off.numpy(), h_t.numpy(), h_v.numpy().view(np.uint32))
+    d_off = h_off.cuda()
+    d_t = h_t.cuda()
+    d_v = h_v.cuda()
+
+    eng = B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
+                    gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block)
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    def device_step():
+        eng.reset()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        eng.push_device(n_event, d_off.data_ptr(), d_t.data_ptr(), d_v.data_ptr())
+        ev1.record(stream)
+        return ev0, ev1
+
+    launches_per_step = 1 + 2  # walk (one bucket here) + 2 finalize kernels
+    from gtpower_b200 import _abi
+    import ctypes as C
+
+    def finalize_device():
+        # finalize kernels only (results stay on the device for the value leg)
+        _abi.check(_abi.lib().gtp_finalize(eng.ctx), eng.ctx)
+
+    for _ in range(args.warmup):
+        device_step()
+        finalize_device()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    kern = []
+    for _ in range(args.steps):
+        kern.append(device_step())
+        finalize_device()
+    s1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = s0.elapsed_time(s1) / args.steps
+    walk_ms = float(np.mean([a.elapsed_time(b) for a, b in kern]))
+
+    # e2e leg: host pinned buffers through the public API, results back to host
+    e2e_ms_list = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.reset()
+        eng.read_power_activities(pinned)
+        res = eng.fetch()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_ms_list.append(a.elapsed_time(b))
+    clocks = sampler.stop()
+    e2e_ms = float(np.mean(e2e_ms_list))
+
+    # max over ranks
+    if pg:
+        t = torch.tensor([step_ms, e2e_ms, walk_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        step_ms, e2e_ms, walk_ms = t.tolist()
+
+    h2d = 8 * (design.n_net + 1) + 8 * n_event + 4 * ((n_event + 15) // 16)
+    d2h = 4 * 5 * design.n_cell + 4 * 5 * eng.n_period + 8 * 5 * 6 + 4
+    b_alg = algorithmic_bytes(design, n_event)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = b_alg / (walk_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic_power_walk.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                tj = json.load(f)
+            traffic = int(tj["bytes_per_launch_scaled"])
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(design, ev, args.cpu_sample_seconds, n_event, tpe)
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": world * n_event / (step_ms / 1e3),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"flat synthetic sky130hd {args.cells} cells x {args.cycles} cycles "
+                                   f"(2 ns, 1 ps ticks, toggle U[0.05,0.3], glitch p=0.05)",
+                       "n_event": n_event, "pin_events": tpe, "n_cell": design.n_cell,
+                       "n_pin": design.n_pin, "n_net": design.n_net, "n_period": eng.n_period,
+                       "cell_cycles_per_s": world * design.n_cell * eng.n_period / (step_ms / 1e3),
+                       "l2": "inputs larger than L2 (event CSR %.2f GB)" % (h2d / 1e9),
+                       "walk_ms": walk_ms, "generation_s": gen_s,
+                       "parallelism": f"weak: {world} independent traces" if world > 1 else "1 GPU"},
+            "e2e": {"value": world * n_event / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "algorithmic_bytes_per_launch": b_alg, "kernel": "power_walk_kernel"},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+            "totals_w": {"leakage": float(res.totals[0]), "internal": float(res.totals[1]),
+                         "switching": float(res.totals[3])},
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+"""ctypes view of the C ABI in include/gtpb200.h.
+
+Loading fails loudly when the compiled library is missing: there is no
+Python or CPU fallback for the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB
+
+GTP_OK = 0
+GTP_GENERAL_ERROR = -1
+GTP_EINVAL = -2
+GTP_ENOMEM = -3
+GTP_ECUDA = -4
+GTP_ETIMEOUT = -5
+GTP_EOVERFLOW = -6
+GTP_ESTATE = -7
+
+STATUS_NAMES = {
+    0: "GTP_OK", -1: "GTP_GENERAL_ERROR", -2: "GTP_EINVAL", -3: "GTP_ENOMEM",
+    -4: "GTP_ECUDA", -5: "GTP_ETIMEOUT", -6: "GTP_EOVERFLOW", -7: "GTP_ESTATE",
+}
+
+GTP_AXIS_NONE, GTP_AXIS_SLEW, GTP_AXIS_CAP = 0, 1, 2
+GROUP_NAMES = ["Combinational", "Sequential", "Clock", "Macro", "Pad"]
+GTP_N_GROUP = 5
+
+
+class gtp_table(C.Structure):
+    _fields_ = [("order", C.c_int32), ("axis1_var", C.c_int32), ("axis2_var", C.c_int32),
+                ("n1", C.c_int32), ("n2", C.c_int32), ("axis1_off", C.c_int64),
+                ("axis2_off", C.c_int64), ("value_off", C.c_int64), ("scale", C.c_float),
+                ("reserved", C.c_int32)]
+
+
+class gtp_when(C.Structure):
+    _fields_ = [("cube_off", C.c_int32), ("n_cube", C.c_int32)]
+
+
+class gtp_internal_power(C.Structure):
+    _fields_ = [("pin", C.c_int32), ("related_pin", C.c_int32), ("when", gtp_when),
+                ("rise_table", C.c_int32), ("fall_table", C.c_int32)]
+
+
+class gtp_leakage_power(C.Structure):
+    _fields_ = [("when", gtp_when), ("power", C.c_float), ("reserved", C.c_int32)]
+
+
+class gtp_cell_type(C.Structure):
+    _fields_ = [("n_pin", C.c_int32), ("n_in", C.c_int32), ("ipwr_off", C.c_int32),
+                ("n_ipwr", C.c_int32), ("leak_off", C.c_int32), ("n_leak", C.c_int32),
+                ("cell_leakage_power", C.c_float), ("has_cell_leakage_power", C.c_int32)]
+
+
+_P = C.c_void_p
+
+
+class gtp_design(C.Structure):
+    _fields_ = [("timescale", C.c_double), ("clk_period", C.c_float), ("reserved0", C.c_int32),
+                ("time_max", C.c_int64),
+                ("n_cell", C.c_int32), ("n_pin", C.c_int32), ("n_net", C.c_int32),
+                ("n_type", C.c_int32),
+                ("cell_pin_off", _P), ("cell_type", _P), ("cell_group", _P), ("cell_arc_off", _P),
+                ("pin_net", _P), ("pin_slew_rise", _P), ("pin_slew_fall", _P),
+                ("pin_load_cap", _P), ("pin_voltage", _P), ("pin_default_state", _P),
+                ("pin_is_clock", _P),
+                ("arc_delay", _P), ("n_arc_delay", C.c_int64),
+                ("types", _P), ("internal_powers", _P), ("leakage_powers", _P), ("tables", _P),
+                ("lut_pool", _P), ("when_cubes", _P),
+                ("n_internal_power", C.c_int32), ("n_leakage_power", C.c_int32),
+                ("n_table", C.c_int32), ("n_when_cube", C.c_int32),
+                ("lut_pool_len", C.c_int64)]
+
+
+class gtp_events(C.Structure):
+    _fields_ = [("n_event", C.c_int64), ("net_off", _P), ("time", _P), ("value_packed", _P),
+                ("net_base", _P), ("t_lo", C.c_int64), ("t_hi", C.c_int64)]
+
+
+class gtp_config(C.Structure):
+    _fields_ = [("cuda_device_id", C.c_int32), ("cycles_per_tile", C.c_int32),
+                ("n_thread_per_block", C.c_int32), ("gates_per_block", C.c_int32),
+                ("max_n_pin_for_leakage_power", C.c_int32), ("collect_counts", C.c_int32),
+                ("max_event_num", C.c_int64), ("reserved", C.c_int64 * 4)]
+
+
+class gtp_counts(C.Structure):
+    _fields_ = [("cell_events", _P), ("cell_glitches", _P), ("cell_half_toggles", _P),
+                ("cell_related", _P), ("cycle_events", _P), ("cycle_glitches", _P),
+                ("dropped", C.c_int64)]
+
+
+# Every symbol the header declares, in order.
+EXPORTED = [
+    "gtp_config_default", "gtp_create", "gtp_destroy", "gtp_last_error", "gtp_n_period",
+    "gtp_ticks_per_cycle", "gtp_reset", "gtp_push_events", "gtp_push_events_device",
+    "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
+    "gtp_pack_values",
+]
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libgtpb200.so (building it first if nvcc is available and the
+    library is missing or stale). Raises if it cannot be loaded."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        try:
+            from .build import build_engine
+            build_engine()
+        except Exception as e:  # pragma: no cover - depends on toolchain
+            raise RuntimeError(f"libgtpb200.so is missing and could not be built: {e}") from e
+    L = C.CDLL(LIB)
+    L.gtp_config_default.argtypes = [C.POINTER(gtp_config)]
+    L.gtp_config_default.restype = None
+    L.gtp_create.argtypes = [C.POINTER(gtp_design), C.POINTER(gtp_config), C.POINTER(C.c_void_p)]
+    L.gtp_create.restype = C.c_int32
+    L.gtp_destroy.argtypes = [C.c_void_p]
+    L.gtp_destroy.restype = None
+    L.gtp_last_error.argtypes = [C.c_void_p]
+    L.gtp_last_error.restype = C.c_char_p
+    L.gtp_n_period.argtypes = [C.c_void_p]
+    L.gtp_n_period.restype = C.c_int64
+    L.gtp_ticks_per_cycle.argtypes = [C.c_void_p]
+    L.gtp_ticks_per_cycle.restype = C.c_int64
+    L.gtp_reset.argtypes = [C.c_void_p]
+    L.gtp_reset.restype = C.c_int32
+    L.gtp_push_events.argtypes = [C.c_void_p, C.POINTER(gtp_events)]
+    L.gtp_push_events.restype = C.c_int32
+    L.gtp_push_events_device.argtypes = [C.c_void_p, C.POINTER(gtp_events)]
+    L.gtp_push_events_device.restype = C.c_int32
+    L.gtp_sync.argtypes = [C.c_void_p]
+    L.gtp_sync.restype = C.c_int32
+    L.gtp_get_stream.argtypes = [C.c_void_p]
+    L.gtp_get_stream.restype = C.c_void_p
+    L.gtp_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.gtp_set_stream.restype = C.c_int32
+    L.gtp_finalize.argtypes = [C.c_void_p]
+    L.gtp_finalize.restype = C.c_int32
+    L.gtp_fetch.argtypes = [C.c_void_p, _P, _P, _P, _P, C.POINTER(gtp_counts)]
+    L.gtp_fetch.restype = C.c_int32
+    L.gtp_pack_values.argtypes = [_P, C.c_int64, _P]
+    L.gtp_pack_values.restype = None
+    _lib = L
+    return L
+
+
+class GtpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def check(status: int, ctx=None) -> None:
+    if status != GTP_OK:
+        msg = lib().gtp_last_error(ctx)
+        raise GtpError(status, msg.decode() if msg else "")

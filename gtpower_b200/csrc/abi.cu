@@ -1,0 +1,471 @@
+// abi.cu — implementation of the C ABI declared in include/gtpb200.h.
+//
+// Replaces the host orchestration of CudaPower::power
+// (power/cuda/CudaPower.cu:1227-1337): the reference allocates a fixed
+// max_event_num AoS buffer, copies it synchronously in full, launches one
+// kernel per interval and merges per-gate tiles. Here a context keeps the
+// packed design resident, copies only the events of each pushed window
+// (asynchronously, on the context's stream), walks them, and keeps the
+// accumulators on the device until gtp_fetch.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "engine.h"
+
+using namespace gtpb;
+
+struct gtp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream in use
+  cudaStream_t own_stream = nullptr;  // created by the context
+  gtp_config cfg;
+  Packed P;
+  std::string err;
+  // static design on device
+  int32_t *d_cell_pin_off = nullptr, *d_cell_type = nullptr, *d_cell_inst = nullptr,
+          *d_order = nullptr, *d_pin_net = nullptr, *d_pin_slot = nullptr;
+  uint8_t *d_pin_flags = nullptr, *d_cell_group = nullptr;
+  float *d_pin_gden = nullptr, *d_pin_swe = nullptr, *d_leak_pool = nullptr, *d_inst = nullptr;
+  DevType* d_types = nullptr;
+  DevSlot* d_slots = nullptr;
+  uint2* d_cubes = nullptr;
+  // events (host-pushed windows)
+  int64_t ev_cap = 0, net_cap_set = 0;
+  int64_t *d_net_off = nullptr, *d_ev_t = nullptr, *d_net_base = nullptr;
+  uint32_t* d_ev_v = nullptr;
+  // accumulators and outputs
+  double* d_cell_acc = nullptr;
+  unsigned long long* d_cyc_acc = nullptr;
+  uint32_t* d_cnt_cell = nullptr;
+  unsigned long long* d_cnt_cyc = nullptr;
+  int32_t* d_status = nullptr;
+  float* d_cell5 = nullptr;
+  float* d_cycle5 = nullptr;
+  double* d_tg = nullptr;
+  unsigned long long* d_leak_tmp = nullptr;
+  double fx_dyn = 0, fx_leak = 0;
+  int64_t last_t_hi = 0;
+  bool any_window = false;
+};
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_create_err;
+
+gtp_status cuda_fail(gtp_ctx* c, cudaError_t e, const char* what) {
+  if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return GTP_ECUDA;
+}
+
+template <typename T>
+cudaError_t upload(T** dst, const std::vector<T>& src, cudaStream_t s) {
+  const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), bytes);
+  if (e != cudaSuccess) return e;
+  if (!src.empty()) e = cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T),
+                                        cudaMemcpyHostToDevice, s);
+  return e;
+}
+
+// largest power of two s with bound * s <= 2^62
+double fixed_point_scale(double bound) {
+  if (!(bound > 0) || !std::isfinite(bound)) return std::ldexp(1.0, 60);
+  int ex;
+  std::frexp(bound, &ex);            // bound < 2^ex
+  return std::ldexp(1.0, 62 - ex);
+}
+
+void free_all(gtp_ctx* c) {
+  void* ptrs[] = {c->d_cell_pin_off, c->d_cell_type, c->d_cell_inst, c->d_order, c->d_pin_net,
+                  c->d_pin_slot, c->d_pin_flags, c->d_cell_group, c->d_pin_gden, c->d_pin_swe,
+                  c->d_leak_pool, c->d_inst, c->d_types, c->d_slots, c->d_cubes, c->d_net_off,
+                  c->d_ev_t, c->d_net_base, c->d_ev_v, c->d_cell_acc, c->d_cyc_acc,
+                  c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
+                  c->d_leak_tmp};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+}
+
+KParams make_params(gtp_ctx* c) {
+  const Packed& P = c->P;
+  KParams k;
+  std::memset(&k, 0, sizeof(k));
+  k.cell_pin_off = c->d_cell_pin_off;
+  k.cell_type = c->d_cell_type;
+  k.cell_inst = c->d_cell_inst;
+  k.order = c->d_order;
+  k.pin_net = c->d_pin_net;
+  k.pin_flags = c->d_pin_flags;
+  k.pin_gden = c->d_pin_gden;
+  k.pin_swe = c->d_pin_swe;
+  k.types = c->d_types;
+  k.slots = c->d_slots;
+  k.pin_slot = c->d_pin_slot;
+  k.cubes = c->d_cubes;
+  k.leak_pool = c->d_leak_pool;
+  k.inst = c->d_inst;
+  k.n_net = P.n_net;
+  k.tpc = P.tpc;
+  k.inv_tpc = 1.0 / static_cast<double>(P.tpc);
+  k.ts = P.ts;
+  k.period_d = P.period_d;
+  k.inv_period_d = 1.0 / P.period_d;
+  k.tmax = P.tmax;
+  k.n_period = P.n_period;
+  k.min_diff0 = static_cast<float>(static_cast<double>(P.tmax) * P.ts);
+  k.fx_dyn = c->fx_dyn;
+  k.fx_leak = c->fx_leak;
+  k.cell_acc = c->d_cell_acc;
+  k.cyc_acc = c->d_cyc_acc;
+  k.cnt_cell = c->d_cnt_cell;
+  k.cnt_cyc = c->d_cnt_cyc;
+  k.n_cell = P.n_cell;
+  k.status = c->d_status;
+  return k;
+}
+
+gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
+                      const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
+                      int64_t t_lo, int64_t t_hi) {
+  if (t_hi <= t_lo) { c->err = "t_hi must exceed t_lo"; return GTP_EINVAL; }
+  if (t_lo < 0) { c->err = "t_lo must be >= 0"; return GTP_EINVAL; }
+  if (c->any_window && t_lo < c->last_t_hi) {
+    c->err = "windows must be pushed in time order without overlap";
+    return GTP_ESTATE;
+  }
+  if (!c->any_window && t_lo != 0) {
+    c->err = "the first window must start at tick 0";
+    return GTP_ESTATE;
+  }
+  const Packed& P = c->P;
+  KParams k = make_params(c);
+  k.net_off = d_net_off;
+  k.ev_t = d_t;
+  k.ev_v = d_v;
+  k.net_base = d_base;
+  k.n_event = n_event;
+  k.t_lo = t_lo;
+  k.t_hi = t_hi;
+  // cycles of the window: [t_lo/tpc, last cycle that can hold an event)
+  const int64_t last_tick = std::min<int64_t>(t_hi - 1, P.tmax);
+  k.cyc0 = t_lo / P.tpc;
+  const int64_t cyc_end = last_tick / P.tpc + 1;
+  const int64_t n_cyc = std::max<int64_t>(1, cyc_end - k.cyc0);
+  int64_t ct = c->cfg.cycles_per_tile;
+  if (ct <= 0) ct = 1024;
+  ct = std::min<int64_t>(ct, n_cyc);
+  const int64_t max_ct = 3072;  // keeps the bins within 227 KB of shared memory
+  ct = std::min(ct, max_ct);
+  ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);  // grid.y limit
+  if (ct > max_ct) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
+  k.cycles_per_tile = ct;
+  k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
+  const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+  k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
+  const bool counts = c->cfg.collect_counts != 0;
+  static const int bucket_pins[3] = {4, 8, kMaxPins};
+  for (int b = 0; b < 3; ++b) {
+    k.order_begin = P.bucket_begin[b];
+    k.order_end = P.bucket_begin[b + 1];
+    if (k.order_end <= k.order_begin) continue;
+    cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "power walk launch");
+  }
+  c->any_window = true;
+  c->last_t_hi = t_hi;
+  return GTP_OK;
+}
+
+gtp_status check_status(gtp_ctx* c) {
+  int32_t st = 0;
+  cudaError_t e = cudaMemcpyAsync(&st, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "status read");
+  if (st) {
+    std::string m = "invalid events:";
+    if (st & kErrNetRange) m += " net_off out of range;";
+    if (st & kErrTimeOrder) m += " times not strictly increasing within a net;";
+    if (st & kErrTimeRange) m += " event time beyond time_max;";
+    if (st & kErrContext) m += " window lacks the event before t_lo for some net;";
+    c->err = m;
+    return GTP_EINVAL;
+  }
+  return GTP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gtp_config_default(gtp_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->cuda_device_id = -1;
+  cfg->cycles_per_tile = 0;
+  cfg->n_thread_per_block = 0;
+  cfg->gates_per_block = 0;
+  cfg->max_n_pin_for_leakage_power = 16;
+  cfg->collect_counts = 0;
+  cfg->max_event_num = 0;  // 0 = no cap other than device memory
+}
+
+gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ctx** out) {
+  if (!out) return GTP_EINVAL;
+  *out = nullptr;
+  auto set_err = [](const std::string& m) {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    g_create_err = m;
+  };
+  if (!design) { set_err("design is NULL"); return GTP_EINVAL; }
+  gtp_ctx* c = new (std::nothrow) gtp_ctx();
+  if (!c) { set_err("out of host memory"); return GTP_ENOMEM; }
+  if (cfg_in) c->cfg = *cfg_in; else gtp_config_default(&c->cfg);
+  if (c->cfg.max_n_pin_for_leakage_power <= 0) c->cfg.max_n_pin_for_leakage_power = 16;
+  std::string err;
+  gtp_status st = pack_design(*design, c->cfg.max_n_pin_for_leakage_power, c->P, err);
+  if (st != GTP_OK) { set_err(err); delete c; return st; }
+
+  cudaError_t e;
+  if (c->cfg.cuda_device_id >= 0) {
+    e = cudaSetDevice(c->cfg.cuda_device_id);
+    if (e != cudaSuccess) { set_err(std::string("cudaSetDevice: ") + cudaGetErrorString(e)); delete c; return GTP_ECUDA; }
+  }
+  cudaGetDevice(&c->device);
+  e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { set_err(std::string("stream: ") + cudaGetErrorString(e)); delete c; return GTP_ECUDA; }
+  c->stream = c->own_stream;
+
+  const Packed& P = c->P;
+  std::vector<uint2> cubes(P.cubes.size() / 2);
+  for (size_t i = 0; i < cubes.size(); ++i) cubes[i] = make_uint2(P.cubes[2 * i], P.cubes[2 * i + 1]);
+#define UP(dst, src) do { e = upload(&c->dst, src, c->stream); if (e != cudaSuccess) goto cuda_err; } while (0)
+  UP(d_cell_pin_off, P.cell_pin_off);
+  UP(d_cell_type, P.cell_type);
+  UP(d_cell_inst, P.cell_inst);
+  UP(d_order, P.order);
+  UP(d_pin_net, P.pin_net);
+  UP(d_pin_slot, P.pin_slot);
+  UP(d_pin_flags, P.pin_flags);
+  UP(d_cell_group, P.cell_group);
+  UP(d_pin_gden, P.pin_gden);
+  UP(d_pin_swe, P.pin_swe);
+  UP(d_leak_pool, P.leak_pool);
+  UP(d_inst, P.inst);
+  UP(d_types, P.types);
+  UP(d_slots, P.slots);
+  UP(d_cubes, cubes);
+#undef UP
+  {
+    const size_t nc = std::max<int32_t>(1, P.n_cell);
+    const size_t ny = static_cast<size_t>(P.n_period + 1);
+    e = cudaMalloc(&c->d_cell_acc, sizeof(double) * kNumCellAcc * nc);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cyc_acc, sizeof(unsigned long long) * kNumCycAcc * ny);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cnt_cell, sizeof(uint32_t) * 4 * nc);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cnt_cyc, sizeof(unsigned long long) * 2 * ny);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_status, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cell5, sizeof(float) * 5 * nc);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cycle5, sizeof(float) * 5 * ny);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_tg, sizeof(double) * (GTP_N_GROUP + 1) * 5);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_leak_tmp, sizeof(unsigned long long) * ny);
+    if (e != cudaSuccess) goto cuda_err;
+  }
+  // fixed-point scales: dynamic energies bounded by max|E| * 2^36 events,
+  // leakage bins by max|leak| * period * 4 * (n_cell + 1)
+  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 36));
+  c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * 4.0 *
+                                 (static_cast<double>(P.n_cell) + 1.0));
+  if (gtp_reset(c) != GTP_OK) { set_err(c->err); free_all(c); delete c; return GTP_ECUDA; }
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) goto cuda_err;
+  *out = c;
+  return GTP_OK;
+cuda_err:
+  set_err(std::string("device setup: ") + cudaGetErrorString(e));
+  free_all(c);
+  delete c;
+  return e == cudaErrorMemoryAllocation ? GTP_ENOMEM : GTP_ECUDA;
+}
+
+void gtp_destroy(gtp_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  delete c;
+}
+
+const char* gtp_last_error(const gtp_ctx* c) {
+  if (c) return c->err.c_str();
+  std::lock_guard<std::mutex> g(g_err_mu);
+  return g_create_err.c_str();
+}
+
+int64_t gtp_n_period(const gtp_ctx* c) { return c ? c->P.n_period : -1; }
+int64_t gtp_ticks_per_cycle(const gtp_ctx* c) { return c ? c->P.tpc : -1; }
+
+gtp_status gtp_reset(gtp_ctx* c) {
+  if (!c) return GTP_EINVAL;
+  const size_t nc = std::max<int32_t>(1, c->P.n_cell);
+  const size_t ny = static_cast<size_t>(c->P.n_period + 1);
+  cudaError_t e = cudaMemsetAsync(c->d_cell_acc, 0, sizeof(double) * kNumCellAcc * nc, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cyc_acc, 0, sizeof(unsigned long long) * kNumCycAcc * ny, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cell, 0, sizeof(uint32_t) * 4 * nc, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cyc, 0, sizeof(unsigned long long) * 2 * ny, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "reset");
+  c->any_window = false;
+  c->last_t_hi = 0;
+  return GTP_OK;
+}
+
+gtp_status gtp_push_events(gtp_ctx* c, const gtp_events* ev) {
+  if (!c || !ev) return GTP_EINVAL;
+  if (ev->n_event < 0 || (ev->n_event > 0 && (!ev->time || !ev->value_packed)) || !ev->net_off) {
+    c->err = "events: missing arrays";
+    return GTP_EINVAL;
+  }
+  const int32_t nn = c->P.n_net;
+  if (ev->net_off[0] != 0 || ev->net_off[nn] != ev->n_event) {
+    c->err = "events: net_off must start at 0 and end at n_event";
+    return GTP_EINVAL;
+  }
+  if (c->cfg.max_event_num > 0 && ev->n_event > c->cfg.max_event_num) {
+    c->err = "events: window exceeds max_event_num";
+    return GTP_EOVERFLOW;
+  }
+  cudaError_t e = cudaSuccess;
+  if (ev->n_event > c->ev_cap || !c->d_net_off) {
+    // grow the event buffers (previous windows are complete once the stream drains)
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+    if (c->d_ev_t) cudaFree(c->d_ev_t);
+    if (c->d_ev_v) cudaFree(c->d_ev_v);
+    c->d_ev_t = nullptr;
+    c->d_ev_v = nullptr;
+    const int64_t cap = std::max<int64_t>(ev->n_event, 16);
+    e = cudaMalloc(&c->d_ev_t, sizeof(int64_t) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_ev_v, sizeof(uint32_t) * ((cap + 15) / 16));
+    if (e != cudaSuccess) {
+      c->ev_cap = 0;
+      c->err = std::string("event buffers: ") + cudaGetErrorString(e);
+      return e == cudaErrorMemoryAllocation ? GTP_ENOMEM : GTP_ECUDA;
+    }
+    c->ev_cap = cap;
+    if (!c->d_net_off) {
+      e = cudaMalloc(&c->d_net_off, sizeof(int64_t) * (nn + 1));
+      if (e == cudaSuccess) e = cudaMalloc(&c->d_net_base, sizeof(int64_t) * std::max(1, nn));
+      if (e != cudaSuccess) return cuda_fail(c, e, "net buffers");
+    }
+  }
+  e = cudaMemcpyAsync(c->d_net_off, ev->net_off, sizeof(int64_t) * (nn + 1), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && ev->n_event > 0)
+    e = cudaMemcpyAsync(c->d_ev_t, ev->time, sizeof(int64_t) * ev->n_event, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && ev->n_event > 0)
+    e = cudaMemcpyAsync(c->d_ev_v, ev->value_packed, sizeof(uint32_t) * ((ev->n_event + 15) / 16),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && ev->net_base)
+    e = cudaMemcpyAsync(c->d_net_base, ev->net_base, sizeof(int64_t) * nn, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "event copy");
+  return run_window(c, c->d_net_off, c->d_ev_t, c->d_ev_v, ev->net_base ? c->d_net_base : nullptr,
+                    ev->n_event, ev->t_lo, ev->t_hi);
+}
+
+gtp_status gtp_push_events_device(gtp_ctx* c, const gtp_events* ev) {
+  if (!c || !ev) return GTP_EINVAL;
+  if (ev->n_event < 0 || !ev->net_off || (ev->n_event > 0 && (!ev->time || !ev->value_packed))) {
+    c->err = "events: missing arrays";
+    return GTP_EINVAL;
+  }
+  return run_window(c, ev->net_off, ev->time, ev->value_packed, ev->net_base, ev->n_event,
+                    ev->t_lo, ev->t_hi);
+}
+
+gtp_status gtp_sync(gtp_ctx* c) {
+  if (!c) return GTP_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+  return check_status(c);
+}
+
+gtp_status gtp_finalize(gtp_ctx* c) {
+  if (!c) return GTP_EINVAL;
+  KParams k = make_params(c);
+  cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
+                                  c->d_leak_tmp, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "finalize");
+  return GTP_OK;
+}
+
+void* gtp_get_stream(const gtp_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+gtp_status gtp_set_stream(gtp_ctx* c, void* stream) {
+  if (!c) return GTP_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return GTP_OK;
+}
+
+gtp_status gtp_fetch(gtp_ctx* c, float* cell5, float* cycle5, double* totals, double* groups,
+                     gtp_counts* counts) {
+  if (!c) return GTP_EINVAL;
+  gtp_status st = check_status(c);
+  if (st != GTP_OK) return st;
+  KParams k = make_params(c);
+  cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
+                                  c->d_leak_tmp, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "finalize");
+  const Packed& P = c->P;
+  const int64_t np = P.n_period;
+  double tg[(GTP_N_GROUP + 1) * 5];
+  if (cell5 && P.n_cell > 0)
+    e = cudaMemcpyAsync(cell5, c->d_cell5, sizeof(float) * 5 * P.n_cell, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && cycle5 && np > 0)
+    e = cudaMemcpyAsync(cycle5, c->d_cycle5, sizeof(float) * 5 * np, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(tg, c->d_tg, sizeof(tg), cudaMemcpyDeviceToHost, c->stream);
+  std::vector<unsigned long long> cyc_cnt;
+  if (e == cudaSuccess && counts) {
+    const int64_t nc = P.n_cell;
+    uint32_t* dst[4] = {counts->cell_events, counts->cell_glitches, counts->cell_half_toggles,
+                        counts->cell_related};
+    for (int q = 0; q < 4 && e == cudaSuccess; ++q)
+      if (dst[q] && nc > 0)
+        e = cudaMemcpyAsync(dst[q], c->d_cnt_cell + q * nc, sizeof(uint32_t) * nc,
+                            cudaMemcpyDeviceToHost, c->stream);
+    cyc_cnt.resize(2 * (np + 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(cyc_cnt.data(), c->d_cnt_cyc, sizeof(unsigned long long) * 2 * (np + 1),
+                          cudaMemcpyDeviceToHost, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "fetch");
+  if (totals) std::memcpy(totals, tg, sizeof(double) * 5);
+  if (groups) std::memcpy(groups, tg + 5, sizeof(double) * 5 * GTP_N_GROUP);
+  if (counts) {
+    for (int64_t y = 0; y < np; ++y) {
+      if (counts->cycle_events) counts->cycle_events[y] = static_cast<int64_t>(cyc_cnt[y]);
+      if (counts->cycle_glitches) counts->cycle_glitches[y] = static_cast<int64_t>(cyc_cnt[np + 1 + y]);
+    }
+    counts->dropped = static_cast<int64_t>(cyc_cnt[np] + cyc_cnt[np + 1 + np]);
+  }
+  return GTP_OK;
+}
+
+void gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed) {
+  const int64_t nw = (n + 15) / 16;
+  for (int64_t w = 0; w < nw; ++w) {
+    uint32_t x = 0;
+    const int64_t b = w * 16;
+    const int64_t m = std::min<int64_t>(16, n - b);
+    for (int64_t j = 0; j < m; ++j) x |= static_cast<uint32_t>(values[b + j] & 3) << (2 * j);
+    packed[w] = x;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+// engine.h — internal data layout shared by the host packer (pack.cpp), the
+// kernels (power_kernel.cu) and the C ABI (abi.cu).
+//
+// Layout in HBM (one context):
+//   static design (uploaded once by gtp_create)
+//     cell_pin_off  int32[n_cell+1]   pins of a cell: inputs, then outputs
+//     cell_type     int32[n_cell]
+//     cell_inst     int32[n_cell]     offset of the cell's energy block in inst[]
+//     order         int32[n_cell]     walk order (cells grouped by pin bucket/type)
+//     pin_net       int32[n_pin]      -1 = no waveform
+//     pin_flags     uint8[n_pin]      bits 0-1 default state, bit 2 is_clock
+//     pin_gden      float[n_pin]      slew_rise + slew_fall (glitch ratio divisor)
+//     pin_swe       float[n_pin]      load_cap * V * V (switching energy per rise)
+//     types/slots/pin_slot/cubes      per-cell-type power program (small)
+//     leak_pool     float[]           2^n_pin leakage table per cell type
+//     inst          float[]           per-instance interpolated energies and arc
+//                                     delays (the NLDM lookups depend only on
+//                                     per-pin slews/caps, so they are done once
+//                                     per instance at create time, in FP32 from
+//                                     FP64 interpolation as the reference does)
+//   events (per pushed window): net_off int64[n_net+1], time int64[E],
+//     value_packed uint32[E/16], net_base int64[n_net] (optional)
+//   accumulators (scratch)
+//     cell_acc  double[5][n_cell]       internal, glitch internal, switching,
+//                                       glitch switching (J), leakage (W*ticks)
+//     cyc_acc   int64[6][n_period+1]    leakage direct, leakage run-difference,
+//                                       internal, glitch internal, switching,
+//                                       glitch switching — 64-bit fixed point
+//                                       energies (J * 2^s), exact and
+//                                       order-independent
+//     cnt_cell  uint32[4][n_cell], cnt_cyc uint64[2][n_period+1] (optional)
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+#include <string>
+
+#include "../../include/gtpb200.h"
+
+namespace gtpb {
+
+// Per cell type program (device copy).
+struct DevType {
+  int32_t n_pin;
+  int32_t n_in;
+  int32_t leak_off;      // into leak_pool; -1 = constant leak_const
+  float   leak_const;
+  int32_t pin_slot_off;  // into pin_slot[]: [n_pin+1] slot index bounds
+  int32_t def_off;       // float offset in the instance block: defaults [n_out][2]
+  int32_t delay_off;     // float offset in the instance block: delays [n_out][n_in][4]
+  int32_t inst_floats;   // floats per instance block
+};
+
+// One internal_power group usable by the walk, in Liberty order per pin.
+struct DevSlot {
+  int32_t related;       // cell-local related input pin, -1 for input-pin groups
+  int32_t cube_off;      // into cubes[] (uint2 care,value)
+  int32_t n_cube;
+  int32_t e_off;         // float offset in the instance block:
+                         //   input pin : [rise, fall]
+                         //   output pin: [from][to] (rise=0, fall=1)
+};
+
+constexpr int kMaxPins = 32;      // cell pins supported by the walk
+constexpr int kNumCycAcc = 6;     // per-cycle fixed-point accumulators
+constexpr int kNumCellAcc = 5;
+
+// Host-side packed design.
+struct Packed {
+  int32_t n_cell = 0, n_pin = 0, n_net = 0;
+  double ts = 0;          // timescale (s/tick)
+  float  period_f = 0;    // clk period (float)
+  double period_d = 0;
+  int64_t tpc = 0;        // ticks per cycle
+  int64_t tmax = 0;
+  int64_t n_period = 0;
+  std::vector<int32_t> cell_pin_off, cell_type, cell_inst, order;
+  std::vector<uint8_t> cell_group;
+  std::vector<int32_t> pin_net;
+  std::vector<uint8_t> pin_flags;
+  std::vector<float>   pin_gden, pin_swe;
+  std::vector<DevType> types;
+  std::vector<DevSlot> slots;
+  std::vector<int32_t> pin_slot;
+  std::vector<uint32_t> cubes;   // pairs
+  std::vector<float>   leak_pool;
+  std::vector<float>   inst;
+  // bucket ranges in order[]: cells with n_pin <= 4, <= 8, <= 32
+  int32_t bucket_begin[4] = {0, 0, 0, 0};
+  double max_abs_energy = 0;     // max |instance energy|, for the fixed-point scale
+  double max_abs_leak = 0;
+};
+
+// Packs and validates a design. Returns GTP_OK or an error with a message.
+gtp_status pack_design(const gtp_design& d, int max_leak_pins, Packed& out, std::string& err);
+
+// Kernel parameter block.
+struct KParams {
+  const int32_t* cell_pin_off;
+  const int32_t* cell_type;
+  const int32_t* cell_inst;
+  const int32_t* order;
+  int32_t order_begin, order_end;
+  const int32_t* pin_net;
+  const uint8_t* pin_flags;
+  const float* pin_gden;
+  const float* pin_swe;
+  const DevType* types;
+  const DevSlot* slots;
+  const int32_t* pin_slot;
+  const uint2* cubes;
+  const float* leak_pool;
+  const float* inst;
+  // events
+  const int64_t* net_off;
+  const int64_t* ev_t;
+  const uint32_t* ev_v;
+  const int64_t* net_base;   // may be null
+  int64_t n_event;
+  int64_t t_lo, t_hi;
+  int32_t n_net;
+  // time base
+  int64_t tpc;
+  double inv_tpc;
+  double ts;
+  double period_d;
+  double inv_period_d;
+  int64_t tmax;
+  int64_t n_period;
+  float min_diff0;           // float(time_max * timescale)
+  // tiling
+  int64_t cyc0;              // first cycle of the window
+  int64_t cycles_per_tile;
+  int32_t n_tiles;
+  int32_t gates_per_block;
+  // fixed point scales (J -> int64)
+  double fx_dyn;
+  double fx_leak;
+  // accumulators
+  double* cell_acc;                 // [5][n_cell]
+  unsigned long long* cyc_acc;      // [6][n_period+1]
+  uint32_t* cnt_cell;               // [4][n_cell]
+  unsigned long long* cnt_cyc;      // [2][n_period+1]
+  int32_t n_cell;
+  int32_t* status;                  // error bits
+};
+
+// status bits set by the kernel
+constexpr int32_t kErrNetRange = 1;
+constexpr int32_t kErrTimeOrder = 2;
+constexpr int32_t kErrTimeRange = 4;
+constexpr int32_t kErrContext = 8;
+
+// Launches the walk over one bucket of cells. shared-memory bytes computed inside.
+cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
+                              cudaStream_t stream);
+size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts);
+
+// Finalize kernels: per-cell floats, totals/groups, per-cycle floats.
+cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,
+                            float* d_cycle5, double* d_totals_groups,
+                            unsigned long long* d_leak_prefix_tmp, cudaStream_t stream);
+
+}  // namespace gtpb

@@ -1,0 +1,383 @@
+// synth.cpp — seeded synthetic designs and traces for the power engine's
+// workloads (host code, no CUDA).
+//
+// Netlist: n_cell cells drawn from a cell mix, levelized as a DAG. Every
+// cell drives one net. A cell's data inputs are wired to nets created
+// earlier (primary inputs, flip-flop outputs, earlier combinational
+// outputs) that still have free fanout slots; each driver gets a fanout
+// target ~ Geometric(p) capped at fanout_cap. Flip-flop clock pins go to
+// one clock net. Wire cap per net ~ lognormal with the given mean and sigma.
+//
+// Trace: a counter-based generator keyed by (seed, net, cycle) so any
+// cycle window of any net can be produced independently and in parallel:
+//   mode 0 (uniform): per-net toggle probability u ~ U[lo, hi];
+//   mode 1 (skew)   : per-net rate ~ Zipf(alpha) over a random net rank,
+//                     scaled to mean `rate_mean`, times a per-cycle burst
+//                     factor ~ lognormal(0, sigma) normalised to mean 1;
+//   mode 2 (phases) : 16-state sticky Markov chain over cycles; each
+//                     (phase, net) pair has its own rate ~ U[lo, hi].
+// A toggle lands at a uniform offset within the cycle; with probability
+// glitch_p it is followed by a pulse of width w ~ U[w_lo, w_hi] ticks (two
+// extra value flips at +w and +2w, kept inside the cycle). The clock net
+// rises at mid-cycle and falls at each later cycle boundary. Every net starts
+// with an event at tick 0 (the VCD initial value); time_max = n_cycle*tpc.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+inline uint64_t splitmix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+inline uint64_t hash3(uint64_t seed, uint64_t a, uint64_t b, uint64_t c) {
+  return splitmix(splitmix(splitmix(seed ^ (a * 0xD6E8FEB86659FD93ull)) ^ (b + 0x632BE59BD9B4E019ull)) ^
+                  (c * 0x9E3779B97F4A7C15ull + 1));
+}
+inline double u01(uint64_t h) { return (h >> 11) * (1.0 / 9007199254740992.0); }
+
+struct Rng {  // sequential generator for netlist construction
+  uint64_t s;
+  explicit Rng(uint64_t seed) : s(seed) {}
+  uint64_t next() { s = splitmix(s); return s; }
+  double uni() { return u01(next()); }
+  int64_t below(int64_t n) { return static_cast<int64_t>(uni() * n) % n; }
+  double normal() {
+    double a = std::max(uni(), 1e-300), b = uni();
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586 * b);
+  }
+};
+
+struct Netlist {
+  std::vector<int32_t> cell_type, cell_pin_off, pin_net;
+  std::vector<double> wire_cap;
+  int32_t n_net = 0;
+  int32_t clock_net = -1;
+  int32_t n_primary_inputs = 0;
+};
+
+struct TraceParams {
+  int64_t n_cycle;
+  int64_t tpc;
+  uint64_t seed;
+  int32_t mode;
+  double lo, hi;             // mode 0 / 2 rate range
+  double zipf_alpha, rate_mean, burst_sigma;  // mode 1
+  int32_t n_phase;           // mode 2
+  double p_stay;             // mode 2
+  double glitch_p;
+  int64_t w_lo, w_hi;
+  int32_t clock_net;
+  int32_t n_net;
+};
+
+struct Trace {
+  TraceParams tp;
+  std::vector<double> net_rate;     // mode 0/1
+  std::vector<uint32_t> rank;       // mode 1
+  std::vector<double> burst;        // mode 1: per cycle factor
+  std::vector<uint8_t> phase;       // mode 2: per cycle phase
+  double prob(int32_t net, int64_t c) const {
+    if (tp.mode == 0) return net_rate[net];
+    if (tp.mode == 1) return std::min(1.0, net_rate[net] * burst[c]);
+    const uint64_t h = hash3(tp.seed ^ 0x5A5A, static_cast<uint64_t>(net), phase[c], 77);
+    return tp.lo + (tp.hi - tp.lo) * u01(h);
+  }
+};
+
+// Events of one net in cycle c; writes up to 3 (time, flip) pairs.
+inline int cycle_events(const Trace& tr, int32_t net, int64_t c, int64_t* t) {
+  const TraceParams& tp = tr.tp;
+  const int64_t base = c * tp.tpc;
+  if (net == tp.clock_net) {  // falls at the cycle boundary, rises mid-cycle
+    if (c == 0) {
+      t[0] = base + tp.tpc / 2;
+      return 1;
+    }
+    t[0] = base;
+    t[1] = base + tp.tpc / 2;
+    return 2;
+  }
+  const uint64_t h = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 1);
+  if (u01(h) >= tr.prob(net, c)) return 0;
+  const uint64_t h2 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 2);
+  const bool glitch = u01(h2) < tp.glitch_p;
+  const uint64_t h3 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 3);
+  const int64_t lo0 = (c == 0) ? 1 : 0;  // tick 0 holds the initial value
+  if (!glitch) {
+    t[0] = base + lo0 + static_cast<int64_t>(u01(h3) * (tp.tpc - lo0));
+    return 1;
+  }
+  const uint64_t h4 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 4);
+  int64_t w = tp.w_lo + static_cast<int64_t>(u01(h4) * (tp.w_hi - tp.w_lo + 1));
+  if (2 * w >= tp.tpc - lo0) w = std::max<int64_t>(1, (tp.tpc - lo0 - 1) / 2);
+  const int64_t span = tp.tpc - lo0 - 2 * w;
+  const int64_t o = lo0 + static_cast<int64_t>(u01(h3) * span);
+  t[0] = base + o;
+  t[1] = base + o + w;
+  t[2] = base + o + 2 * w;
+  return 3;
+}
+
+}  // namespace
+
+extern "C" {
+
+// cell mix: fraction per type, n_in per type (data inputs, clock counted
+// separately through is_ff). Pins of a cell: inputs in type order, then the
+// single output.
+void* synth_netlist_create(int64_t n_cell, uint64_t seed, int32_t n_type, const double* mix,
+                           const int32_t* type_n_in, const int32_t* type_is_ff,
+                           double fanout_p, int32_t fanout_cap, double wire_mean,
+                           double wire_sigma, double pi_fraction) {
+  Netlist* nl = new Netlist();
+  Rng rng(seed * 0x2545F4914F6CDD1Dull + 17);
+  // exact type counts from the mix, then a seeded shuffle
+  std::vector<int32_t> types;
+  types.reserve(n_cell);
+  double acc = 0;
+  int64_t assigned = 0;
+  for (int32_t t = 0; t < n_type; ++t) {
+    acc += mix[t];
+    const int64_t upto = (t == n_type - 1) ? n_cell : static_cast<int64_t>(std::llround(acc * n_cell));
+    for (; assigned < upto; ++assigned) types.push_back(t);
+  }
+  for (int64_t i = n_cell - 1; i > 0; --i) std::swap(types[i], types[rng.below(i + 1)]);
+  nl->cell_type = types;
+
+  // nets: clock, primary inputs, then one output net per cell (net id = n_pre + cell)
+  const int32_t n_pi = std::max<int32_t>(16, static_cast<int32_t>(pi_fraction * n_cell));
+  nl->clock_net = 0;
+  nl->n_primary_inputs = n_pi;
+  const int32_t n_pre = 1 + n_pi;
+  nl->n_net = n_pre + static_cast<int32_t>(n_cell);
+  std::vector<int32_t> slots(nl->n_net, 0);
+  auto fanout_target = [&]() {
+    int k = 1;
+    while (k < fanout_cap && rng.uni() >= fanout_p) ++k;
+    return k;
+  };
+  std::vector<int32_t> open;  // nets with free fanout slots
+  open.reserve(nl->n_net);
+  for (int32_t n = 1; n < n_pre; ++n) { slots[n] = fanout_target(); open.push_back(n); }
+  // flip-flop outputs exist from the start (sequential boundary)
+  for (int64_t c = 0; c < n_cell; ++c)
+    if (type_is_ff[types[c]]) {
+      const int32_t net = n_pre + static_cast<int32_t>(c);
+      slots[net] = fanout_target();
+      open.push_back(net);
+    }
+  auto take = [&]() -> int32_t {
+    if (open.empty()) {  // add a primary input on demand
+      const int32_t net = nl->n_net++;
+      slots.push_back(fanout_target());
+      open.push_back(net);
+      ++nl->n_primary_inputs;
+    }
+    const int64_t k = rng.below(static_cast<int64_t>(open.size()));
+    const int32_t net = open[k];
+    if (--slots[net] == 0) { open[k] = open.back(); open.pop_back(); }
+    return net;
+  };
+  nl->cell_pin_off.resize(n_cell + 1);
+  nl->cell_pin_off[0] = 0;
+  // flip-flop data inputs are wired last (they may take any driver)
+  std::vector<std::vector<int32_t>> pins(n_cell);
+  for (int64_t c = 0; c < n_cell; ++c) {
+    const int32_t t = types[c];
+    const int32_t n_in = type_n_in[t];
+    std::vector<int32_t>& p = pins[c];
+    p.assign(n_in + 1, -1);
+    if (!type_is_ff[t]) {
+      for (int32_t i = 0; i < n_in; ++i) p[i] = take();
+      const int32_t net = n_pre + static_cast<int32_t>(c);
+      slots[net] = fanout_target();
+      open.push_back(net);
+    }
+    p[n_in] = n_pre + static_cast<int32_t>(c);
+  }
+  for (int64_t c = 0; c < n_cell; ++c) {
+    const int32_t t = types[c];
+    if (!type_is_ff[t]) continue;
+    const int32_t n_in = type_n_in[t];
+    pins[c][0] = nl->clock_net;                    // CLK
+    for (int32_t i = 1; i < n_in; ++i) pins[c][i] = take();
+  }
+  for (int64_t c = 0; c < n_cell; ++c) {
+    nl->cell_pin_off[c + 1] = nl->cell_pin_off[c] + static_cast<int32_t>(pins[c].size());
+    nl->pin_net.insert(nl->pin_net.end(), pins[c].begin(), pins[c].end());
+  }
+  // wire caps: lognormal with the requested mean
+  nl->wire_cap.resize(nl->n_net);
+  const double mu = std::log(wire_mean) - 0.5 * wire_sigma * wire_sigma;
+  for (int32_t n = 0; n < nl->n_net; ++n) nl->wire_cap[n] = std::exp(mu + wire_sigma * rng.normal());
+  return nl;
+}
+
+int64_t synth_netlist_size(void* h, int32_t which) {
+  Netlist* nl = static_cast<Netlist*>(h);
+  switch (which) {
+    case 0: return static_cast<int64_t>(nl->cell_type.size());
+    case 1: return static_cast<int64_t>(nl->pin_net.size());
+    case 2: return nl->n_net;
+    case 3: return nl->clock_net;
+    case 4: return nl->n_primary_inputs;
+  }
+  return -1;
+}
+
+void synth_netlist_copy(void* h, int32_t* cell_type, int32_t* cell_pin_off, int32_t* pin_net,
+                        double* wire_cap) {
+  Netlist* nl = static_cast<Netlist*>(h);
+  std::memcpy(cell_type, nl->cell_type.data(), sizeof(int32_t) * nl->cell_type.size());
+  std::memcpy(cell_pin_off, nl->cell_pin_off.data(), sizeof(int32_t) * nl->cell_pin_off.size());
+  std::memcpy(pin_net, nl->pin_net.data(), sizeof(int32_t) * nl->pin_net.size());
+  std::memcpy(wire_cap, nl->wire_cap.data(), sizeof(double) * nl->wire_cap.size());
+}
+
+void synth_netlist_free(void* h) { delete static_cast<Netlist*>(h); }
+
+void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int64_t tpc,
+                         uint64_t seed, int32_t mode, double lo, double hi, double zipf_alpha,
+                         double rate_mean, double burst_sigma, int32_t n_phase, double p_stay,
+                         double glitch_p, int64_t w_lo, int64_t w_hi) {
+  Trace* tr = new Trace();
+  TraceParams& tp = tr->tp;
+  tp.n_cycle = n_cycle; tp.tpc = tpc; tp.seed = seed; tp.mode = mode;
+  tp.lo = lo; tp.hi = hi; tp.zipf_alpha = zipf_alpha; tp.rate_mean = rate_mean;
+  tp.burst_sigma = burst_sigma; tp.n_phase = n_phase; tp.p_stay = p_stay;
+  tp.glitch_p = glitch_p; tp.w_lo = w_lo; tp.w_hi = w_hi; tp.clock_net = clock_net;
+  tp.n_net = n_net;
+  Rng rng(seed ^ 0x1234567ull);
+  if (mode == 0) {
+    tr->net_rate.resize(n_net);
+    for (int32_t n = 0; n < n_net; ++n)
+      tr->net_rate[n] = lo + (hi - lo) * u01(hash3(seed, n, 0xFFFFFFFFull, 9));
+  } else if (mode == 1) {
+    // Zipf over a random rank permutation, scaled to the requested mean
+    std::vector<uint32_t> perm(n_net);
+    for (int32_t n = 0; n < n_net; ++n) perm[n] = n;
+    for (int32_t i = n_net - 1; i > 0; --i) std::swap(perm[i], perm[rng.below(i + 1)]);
+    tr->net_rate.resize(n_net);
+    double sum = 0;
+    for (int32_t n = 0; n < n_net; ++n) {
+      tr->net_rate[n] = 1.0 / std::pow(static_cast<double>(perm[n]) + 1.0, zipf_alpha);
+      sum += tr->net_rate[n];
+    }
+    const double k = rate_mean * n_net / sum;
+    for (int32_t n = 0; n < n_net; ++n) tr->net_rate[n] = std::min(1.0, tr->net_rate[n] * k);
+    tr->burst.resize(n_cycle);
+    double bs = 0;
+    for (int64_t c = 0; c < n_cycle; ++c) {
+      tr->burst[c] = std::exp(burst_sigma * rng.normal());
+      bs += tr->burst[c];
+    }
+    const double m = bs / std::max<int64_t>(1, n_cycle);
+    for (int64_t c = 0; c < n_cycle; ++c) tr->burst[c] /= m;
+  } else {
+    tr->phase.resize(n_cycle);
+    uint8_t ph = static_cast<uint8_t>(rng.below(n_phase));
+    for (int64_t c = 0; c < n_cycle; ++c) {
+      if (rng.uni() >= p_stay) ph = static_cast<uint8_t>(rng.below(n_phase));
+      tr->phase[c] = ph;
+    }
+  }
+  return tr;
+}
+
+void synth_trace_free(void* h) { delete static_cast<Trace*>(h); }
+
+int32_t synth_trace_phase(void* h, int64_t c) {
+  Trace* tr = static_cast<Trace*>(h);
+  return tr->phase.empty() ? -1 : tr->phase[c];
+}
+
+// Events of every net for cycles [c_lo, c_hi), plus the tick-0 initial value
+// when c_lo == 0. counts[n] receives the count per net.
+void synth_trace_count(void* h, int64_t c_lo, int64_t c_hi, int64_t* counts, int32_t n_threads) {
+  Trace* tr = static_cast<Trace*>(h);
+  const int32_t nn = tr->tp.n_net;
+  if (n_threads < 1) n_threads = 1;
+  auto job = [&](int tid) {
+    int64_t t[3];
+    for (int32_t n = tid; n < nn; n += n_threads) {
+      int64_t k = (c_lo == 0) ? 1 : 0;
+      for (int64_t c = c_lo; c < c_hi; ++c) k += cycle_events(*tr, n, c, t);
+      counts[n] = k;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 0; i < n_threads; ++i) th.emplace_back(job, i);
+  for (auto& x : th) x.join();
+}
+
+// Fills times and one value byte per event (0/1) for cycles [c_lo, c_hi).
+// init_value[n] is the net's value before c_lo (updated in place to the
+// value after c_hi). off[n] is where net n's events start.
+void synth_trace_fill(void* h, int64_t c_lo, int64_t c_hi, const int64_t* off,
+                      uint8_t* init_value, int64_t* times, uint8_t* values, int32_t n_threads) {
+  Trace* tr = static_cast<Trace*>(h);
+  const int32_t nn = tr->tp.n_net;
+  if (n_threads < 1) n_threads = 1;
+  auto job = [&](int tid) {
+    int64_t t[3];
+    for (int32_t n = tid; n < nn; n += n_threads) {
+      int64_t k = off[n];
+      uint8_t v = init_value[n];
+      if (c_lo == 0) {
+        times[k] = 0;
+        values[k] = v;
+        ++k;
+      }
+      for (int64_t c = c_lo; c < c_hi; ++c) {
+        const int m = cycle_events(*tr, n, c, t);
+        for (int j = 0; j < m; ++j) {
+          v ^= 1;
+          times[k] = t[j];
+          values[k] = v;
+          ++k;
+        }
+      }
+      init_value[n] = v;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 0; i < n_threads; ++i) th.emplace_back(job, i);
+  for (auto& x : th) x.join();
+}
+
+// Packs one value per byte into 2-bit fields, 16 per uint32 word, with
+// n_threads threads over word ranges.
+void synth_pack_values(const uint8_t* values, int64_t n, uint32_t* packed, int32_t n_threads) {
+  const int64_t nw = (n + 15) / 16;
+  if (n_threads < 1) n_threads = 1;
+  auto job = [&](int tid) {
+    const int64_t per = (nw + n_threads - 1) / n_threads;
+    const int64_t w0 = tid * per, w1 = std::min(nw, w0 + per);
+    for (int64_t w = w0; w < w1; ++w) {
+      uint32_t x = 0;
+      const int64_t b = w * 16;
+      const int64_t m = std::min<int64_t>(16, n - b);
+      for (int64_t j = 0; j < m; ++j) x |= static_cast<uint32_t>(values[b + j] & 3) << (2 * j);
+      packed[w] = x;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 0; i < n_threads; ++i) th.emplace_back(job, i);
+  for (auto& x : th) x.join();
+}
+
+// Initial net values (tick 0): a seeded coin per net; the clock starts at 0.
+void synth_trace_initial(void* h, uint8_t* init_value) {
+  Trace* tr = static_cast<Trace*>(h);
+  for (int32_t n = 0; n < tr->tp.n_net; ++n)
+    init_value[n] = (n == tr->tp.clock_net) ? 0 : static_cast<uint8_t>(hash3(tr->tp.seed, n, 0xABCDEFull, 5) & 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,280 @@
+/*
+ * gtpb200.h — C ABI of the B200 time-based power engine.
+ *
+ * This is the drop-in boundary for GTPower's time-based power path. The
+ * reference exposes that path as the C++ virtual interface
+ *
+ *   gtpower::Power::power(corner, total, sequential, combinational,
+ *                         clock, macro, pad)          power/Power.hh:80-87
+ *   gtpower::Power::printCellRes()                    power/Power.hh:109
+ *
+ * implemented on the CPU by Power::power (power/Power.cc:227-386) and
+ * findTimeBasedAllPower (power/TimeBasedPower.cc:703-901), and on CUDA by
+ * CudaPower::power (power/cuda/CudaPower.cu:1227-1337). Waveforms reach it
+ * through Power::setUserActivity(pin, ..., const VcdValues*, value_bit)
+ * (power/Power.cc:138-147).
+ *
+ * The ABI below carries the same information as plain arrays:
+ *   - gtp_design: what CudaPower::initGateData gathers from OpenSTA per pin
+ *     and per cell (power/cuda/CudaPower.cu:1601-1816): slews, load caps,
+ *     voltages, default states, clock flags, arc delays, and the Liberty
+ *     internal_power / leakage_power groups of every cell type;
+ *   - gtp_events: the per-net event list (tick, value) that the reference
+ *     keeps as VcdValues per var/bit (power/Vcd.hh, power/Vcd.cc:204-277),
+ *     as a CSR over nets;
+ *   - gtp_fetch: per-cell values (the rows of cuda_cell_power.txt,
+ *     power/cuda/CudaPower.cu:3134-3165), per-cycle waveforms (the sections
+ *     of cuda_per_cycle_waveform.txt, include/sta/PowerClass.hh:123-149) and
+ *     the report_power group totals (power/Power.cc:330-347).
+ *
+ * All pointers are host pointers unless the name starts with d_. No call
+ * keeps a pointer to caller memory after it returns. One context per host
+ * thread; a context owns its CUDA streams and device memory.
+ */
+#ifndef GTPB200_H
+#define GTPB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. GTP_OK and GTP_GENERAL_ERROR keep the values of the
+ * reference's ErrorCode (OK=0, GENERAL_ERROR=-1); the reference itself exits
+ * the process on errors (util/Log.hh:58-60, util/cuda/CheckCudaRuntime.cu). */
+typedef int32_t gtp_status;
+#define GTP_OK             0
+#define GTP_GENERAL_ERROR (-1)
+#define GTP_EINVAL        (-2)   /* malformed design or events            */
+#define GTP_ENOMEM        (-3)   /* host or device allocation failed       */
+#define GTP_ECUDA         (-4)   /* CUDA runtime error                     */
+#define GTP_ETIMEOUT      (-5)   /* a bounded device wait gave up          */
+#define GTP_EOVERFLOW     (-6)   /* a size exceeds a documented limit      */
+#define GTP_ESTATE        (-7)   /* calls made in the wrong order          */
+
+/* Pin values, as Power::vcd_value_to_int_map_ (power/Power.hh:114). */
+#define GTP_V0 0
+#define GTP_V1 1
+#define GTP_VX 2
+#define GTP_VZ 3
+
+/* Report groups, as Power::power classifies instances
+ * (power/Power.cc:338-347: macro, pad, clock network, sequential, else
+ * combinational). */
+#define GTP_GROUP_COMBINATIONAL 0
+#define GTP_GROUP_SEQUENTIAL    1
+#define GTP_GROUP_CLOCK         2
+#define GTP_GROUP_MACRO         3
+#define GTP_GROUP_PAD           4
+#define GTP_N_GROUP             5
+
+/* Table axis variables (liberty/InternalPower.cc:215-228). */
+#define GTP_AXIS_NONE 0
+#define GTP_AXIS_SLEW 1   /* input_transition_time          */
+#define GTP_AXIS_CAP  2   /* total_output_net_capacitance   */
+
+/* One NLDM power table (rise_power or fall_power of an internal_power
+ * group): liberty/TableModel.cc Table0/Table1/Table2. Values are SI (J);
+ * axes are SI (s, F). values are row-major [n1][n2]. */
+typedef struct gtp_table {
+  int32_t order;          /* 0, 1 or 2 */
+  int32_t axis1_var;      /* GTP_AXIS_* */
+  int32_t axis2_var;
+  int32_t n1, n2;         /* axis sizes (1 for unused axes) */
+  int64_t axis1_off;      /* offsets into gtp_design.lut_pool */
+  int64_t axis2_off;
+  int64_t value_off;
+  float   scale;          /* TableModel::scaleFactor (1.0 if none) */
+  int32_t reserved;
+} gtp_table;
+
+/* A `when` condition in disjunctive normal form over the cell's pins: it
+ * holds when, for some cube k, (ones & care[k]) == value[k], where bit i of
+ * `ones` is set iff pin i is in state 1 (X and Z count as not-one, as
+ * evalWhen does in power/PowerUtils.cc:153-186). A group without `when`
+ * is one cube with care = 0. Zero cubes = never true. */
+typedef struct gtp_when {
+  int32_t cube_off;       /* into gtp_design.when_cubes (pairs care,value) */
+  int32_t n_cube;
+} gtp_when;
+
+/* A Liberty internal_power group of one cell type, in Liberty order
+ * (LibertyCell::internalPowers; used by findInputInternalVal and
+ * findOutputInternalVal, power/TimeBasedPower.cc:341-509). */
+typedef struct gtp_internal_power {
+  int32_t  pin;           /* cell-local pin index of the group's port */
+  int32_t  related_pin;   /* cell-local related pin index, -1 if none */
+  gtp_when when;
+  int32_t  rise_table;    /* index into gtp_design.tables, -1 if absent */
+  int32_t  fall_table;
+} gtp_internal_power;
+
+/* A Liberty leakage_power group, in Liberty order
+ * (Power::getLeakagePower, power/TimeBasedPower.cc:258-301). The reference
+ * expands only conjunctions (getWhenPinStates, power/PowerUtils.cc:191-201);
+ * an unsupported or unsatisfiable `when` is encoded with n_cube = 0. */
+typedef struct gtp_leakage_power {
+  gtp_when when;
+  float    power;         /* W */
+  int32_t  reserved;
+} gtp_leakage_power;
+
+/* A library cell type. Pins are ordered inputs first, then outputs, in
+ * instance pin-iterator order (Power::getPinInformation,
+ * power/TimeBasedPower.cc:223-256). */
+typedef struct gtp_cell_type {
+  int32_t n_pin;
+  int32_t n_in;
+  int32_t ipwr_off, n_ipwr;   /* into gtp_design.internal_powers */
+  int32_t leak_off, n_leak;   /* into gtp_design.leakage_powers  */
+  float   cell_leakage_power; /* cell_leakage_power attribute (W) */
+  int32_t has_cell_leakage_power;
+} gtp_cell_type;
+
+/* The static design: everything the power walk reads besides the events. */
+typedef struct gtp_design {
+  /* time base */
+  double  timescale;      /* seconds per VCD tick (Vcd::timeScale)        */
+  float   clk_period;     /* seconds, as float (Power::clk_period_)       */
+  int32_t reserved0;
+  int64_t time_max;       /* last VCD timestamp (Vcd::timeMax)            */
+
+  int32_t n_cell, n_pin, n_net, n_type;
+
+  /* cells */
+  const int32_t* cell_pin_off;   /* [n_cell+1] */
+  const int32_t* cell_type;      /* [n_cell]   */
+  const uint8_t* cell_group;     /* [n_cell]   GTP_GROUP_*  */
+  const int64_t* cell_arc_off;   /* [n_cell]   offset into arc_delay        */
+
+  /* pins */
+  const int32_t* pin_net;        /* [n_pin] net id; -1 = no waveform        */
+  const float*   pin_slew_rise;  /* [n_pin] s; +inf = no slew (delayInf)    */
+  const float*   pin_slew_fall;  /* [n_pin] s                               */
+  const float*   pin_load_cap;   /* [n_pin] F (GraphDelayCalc::loadCap)     */
+  const float*   pin_voltage;    /* [n_pin] V (Power::portVoltage)          */
+  const uint8_t* pin_default_state; /* [n_pin] 0/1/2, for pins w/o events   */
+  const uint8_t* pin_is_clock;   /* [n_pin] LibertyPort::isClock            */
+
+  /* arc delays: per cell [n_out][n_in][4] floats (s), arc index
+   * 2*(from==fall)+(to==fall) as Gate::cellArcDelay
+   * (power/cuda/Gate.cuh:344-348); NaN = no timing arc. */
+  const float*   arc_delay;
+  int64_t        n_arc_delay;
+
+  /* library */
+  const gtp_cell_type*      types;            /* [n_type] */
+  const gtp_internal_power* internal_powers;  /* [n_internal_power] */
+  const gtp_leakage_power*  leakage_powers;   /* [n_leakage_power] */
+  const gtp_table*          tables;           /* [n_table] */
+  const float*              lut_pool;         /* [lut_pool_len] */
+  const uint32_t*           when_cubes;       /* [2*n_when_cube] */
+  int32_t n_internal_power, n_leakage_power, n_table, n_when_cube;
+  int64_t lut_pool_len;
+} gtp_design;
+
+/* Per-net event lists for one window of time, CSR over nets.
+ * Events with time in [t_lo, t_hi) are processed; events outside it are
+ * context. A window after the first must list, for every net, all events of
+ * the last clock period that has an event before t_lo plus the event before
+ * that period, and the first two events at or after t_hi (when they exist):
+ * glitch classification and related-pin search look that far. A single
+ * window over the whole trace (t_lo = 0, t_hi = INT64_MAX, net_base = NULL)
+ * needs no context. */
+typedef struct gtp_events {
+  int64_t         n_event;
+  const int64_t*  net_off;       /* [n_net+1] */
+  const int64_t*  time;          /* [n_event] ticks, strictly increasing per net */
+  const uint32_t* value_packed;  /* [ceil(n_event/16)] 2 bits per event, event
+                                    i in word i/16 at bit 2*(i%16) */
+  const int64_t*  net_base;      /* [n_net] index, within the net's whole
+                                    waveform, of its first listed event; NULL = 0 */
+  int64_t t_lo, t_hi;
+} gtp_events;
+
+/* Tunables. Field names follow util/GlobalConfig.hh where one exists. */
+typedef struct gtp_config {
+  int32_t cuda_device_id;            /* -1 = current device */
+  int32_t cycles_per_tile;           /* cycle tile of one CTA; 0 = auto */
+  int32_t n_thread_per_block;        /* 0 = auto */
+  int32_t gates_per_block;           /* gates one CTA walks per tile; 0 = auto */
+  int32_t max_n_pin_for_leakage_power; /* 16 (GlobalConfig.hh:41) */
+  int32_t collect_counts;            /* 1 = fill gtp_counts (exact parity) */
+  int64_t max_event_num;             /* device event capacity (GlobalConfig.hh:31) */
+  int64_t reserved[4];
+} gtp_config;
+
+/* Integer counters that must match the oracle bit-exactly. */
+typedef struct gtp_counts {
+  uint32_t* cell_events;       /* [n_cell] pin events walked                 */
+  uint32_t* cell_glitches;     /* [n_cell] events classified as glitch       */
+  uint32_t* cell_half_toggles; /* [n_cell] sum of 2*n_toggle                 */
+  uint32_t* cell_related;      /* [n_cell] sum over output events of
+                                  (related input pin + 1), 0 for default     */
+  int64_t*  cycle_events;      /* [n_period] pin events per cycle            */
+  int64_t*  cycle_glitches;    /* [n_period] glitch events per cycle         */
+  int64_t   dropped;           /* contributions past the last cycle          */
+} gtp_counts;
+
+typedef struct gtp_ctx gtp_ctx;
+
+void        gtp_config_default(gtp_config* cfg);
+
+/* Validates and packs the design, uploads it to the device. */
+gtp_status  gtp_create(const gtp_design* design, const gtp_config* cfg, gtp_ctx** out);
+void        gtp_destroy(gtp_ctx* ctx);
+const char* gtp_last_error(const gtp_ctx* ctx);
+
+/* Number of per-cycle entries: ceil(time_max*timescale/clk_period), as
+ * Power::power sizes its waveforms (power/Power.cc:248). */
+int64_t     gtp_n_period(const gtp_ctx* ctx);
+/* Ticks per clock cycle: (int64)ceil(float(clk_period)/float(timescale)),
+ * as clkedWaveformIdx (power/PowerUtils.cc:27-32). */
+int64_t     gtp_ticks_per_cycle(const gtp_ctx* ctx);
+
+/* Clears all accumulators (start of a new trace). */
+gtp_status  gtp_reset(gtp_ctx* ctx);
+
+/* Copies one window of events from host memory (pinned or pageable) to the
+ * device and evaluates it. Windows must come in time order. */
+gtp_status  gtp_push_events(gtp_ctx* ctx, const gtp_events* ev);
+
+/* Same, with events already in device memory (time, value_packed, net_off,
+ * net_base are device pointers). Nothing is copied. */
+gtp_status  gtp_push_events_device(gtp_ctx* ctx, const gtp_events* d_ev);
+
+/* Waits for all queued work. */
+gtp_status  gtp_sync(gtp_ctx* ctx);
+
+/* The cudaStream_t (as void*) all of the context's work is queued on.
+ * gtp_set_stream replaces it with a caller-owned stream (NULL restores the
+ * context's own); the caller keeps ownership and must keep it alive. */
+void*       gtp_get_stream(const gtp_ctx* ctx);
+gtp_status  gtp_set_stream(gtp_ctx* ctx, void* stream);
+
+/* Queues the kernels that turn the accumulators into the outputs of
+ * gtp_fetch, without waiting (gtp_fetch runs them too). */
+gtp_status  gtp_finalize(gtp_ctx* ctx);
+
+/* Results. Any pointer may be NULL.
+ * cell5   [n_cell][5]   : Internal_Power, Glitch_Internal_Power,
+ *                         Switching_Power, Glitch_Switching_Power,
+ *                         Leakage_Power (W; "Internal"/"Switching" exclude
+ *                         glitch, as the columns of cuda_cell_power.txt)
+ * cycle5  [5][n_period] : leakage, internal (incl. glitch), glitch internal,
+ *                         switching (incl. glitch), glitch switching (W), the
+ *                         sections of cuda_per_cycle_waveform.txt
+ * totals  [5]           : design totals in FP64, same order as cycle5
+ * groups  [GTP_N_GROUP][5] : per report group, FP64, same order as cycle5
+ */
+gtp_status  gtp_fetch(gtp_ctx* ctx, float* cell5, float* cycle5,
+                      double* totals, double* groups, gtp_counts* counts);
+
+/* Packs one value per byte (0..3) into the 2-bit layout of value_packed. */
+void        gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GTPB200_H */

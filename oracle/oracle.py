@@ -1,0 +1,101 @@
+"""ctypes binding of the CPU oracle (oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline legs, never by the gtpower_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "oracle.cpp")
+    hdr = os.path.join(os.path.dirname(HERE), "include", "gtpb200.h")
+    if force or not os.path.exists(LIB) or max(os.path.getmtime(src), os.path.getmtime(hdr)) > os.path.getmtime(LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "_build/liboracle.so"], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        L.oracle_run.restype = C.c_int
+        L.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int, C.c_int,
+                                 C.c_int] + [C.c_void_p] * 11 + [C.POINTER(C.c_double)]
+        L.oracle_n_period.restype = C.c_int64
+        L.oracle_n_period.argtypes = [C.c_void_p]
+        L.oracle_ticks_per_cycle.restype = C.c_int64
+        L.oracle_ticks_per_cycle.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+@dataclass
+class OracleResult:
+    cell5: np.ndarray        # [n_cell, 5] internal, glitch internal, switching, glitch switching, leakage
+    cycle5: np.ndarray       # [5, n_period] leakage, internal, glitch internal, switching, glitch switching
+    totals: np.ndarray       # [5] same order as cycle5
+    groups: np.ndarray       # [5 groups, 5]
+    cell_events: np.ndarray
+    cell_glitches: np.ndarray
+    cell_half_toggles: np.ndarray
+    cell_related: np.ndarray
+    cycle_events: np.ndarray
+    cycle_glitches: np.ndarray
+    dropped: int
+    seconds: float
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def run(design, events, fp32: bool = False, threads: int = 1, cells: np.ndarray | None = None,
+        max_leak_pins: int = 16, outputs: bool = True) -> OracleResult:
+    """Runs the restated reference CPU path over `events` (one whole-trace
+    window). fp32=False is the FP64 oracle; fp32=True is the reference's own
+    FP32 arithmetic (the timed CPU baseline)."""
+    L = lib()
+    d = design.c_struct()
+    e = events.c_struct()
+    n_cell = design.n_cell
+    npd = int(L.oracle_n_period(C.byref(d)))
+    cell5 = np.zeros((n_cell, 5))
+    cyc5 = np.zeros((5, max(npd, 0)))
+    tot = np.zeros(5)
+    grp = np.zeros((5, 5))
+    ce = np.zeros(n_cell, dtype=np.uint32)
+    cg = np.zeros(n_cell, dtype=np.uint32)
+    ch = np.zeros(n_cell, dtype=np.uint32)
+    cr = np.zeros(n_cell, dtype=np.uint32)
+    ye = np.zeros(max(npd, 0), dtype=np.int64)
+    yg = np.zeros(max(npd, 0), dtype=np.int64)
+    dropped = np.zeros(1, dtype=np.int64)
+    secs = C.c_double(0)
+    sel = None
+    n_sel = 0
+    if cells is not None:
+        sel = np.ascontiguousarray(cells, dtype=np.int32)
+        n_sel = sel.shape[0]
+    o = outputs
+    rc = L.oracle_run(C.byref(d), C.byref(e), _p(sel) if sel is not None else None, n_sel,
+                      threads, 1 if fp32 else 0, max_leak_pins,
+                      _p(cell5) if o else None, _p(cyc5) if o else None, _p(tot), _p(grp),
+                      _p(ce) if o else None, _p(cg) if o else None, _p(ch) if o else None,
+                      _p(cr) if o else None, _p(ye) if o else None, _p(yg) if o else None,
+                      _p(dropped), C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"oracle_run failed: {rc}")
+    return OracleResult(cell5, cyc5, tot, grp, ce, cg, ch, cr, ye, yg, int(dropped[0]), secs.value)

@@ -1,0 +1,67 @@
+"""GPU parity: the CUDA engine against the FP64 oracle on the same inputs."""
+import numpy as np
+import pytest
+
+from tests import toy
+from tests.parity import compare
+
+pytestmark = pytest.mark.gpu
+
+
+def run_engine(design, windows, **kw):
+    from gtpower_b200 import B200Power
+    with B200Power(design, collect_counts=True, **kw) as eng:
+        for w in windows:
+            eng.read_power_activities(w)
+        eng.sync()
+        return eng.fetch(counts=True)
+
+
+def oracle(design, events):
+    from oracle import oracle as orc
+    return orc.run(design, events)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+@pytest.mark.parametrize("cycles_per_tile", [0, 3, 17])
+def test_random_toy_designs(seed, cycles_per_tile):
+    rng = np.random.default_rng(seed)
+    d, ev = toy.random_design(rng, n_cell=300, n_net=120, time_max=20_000, tpc=700)
+    res = run_engine(d, [ev], cycles_per_tile=cycles_per_tile)
+    compare(res, oracle(d, ev))
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_random_toy_windows(seed):
+    from gtpower_b200 import windows
+    rng = np.random.default_rng(seed)
+    d, ev = toy.random_design(rng, n_cell=200, n_net=90, time_max=15_000, tpc=500)
+    tpc = d.ticks_per_cycle
+    wins = windows.split(ev, tpc, [0, 3, 11, 12, 20, 31])
+    res = run_engine(d, wins, cycles_per_tile=4)
+    compare(res, oracle(d, ev))
+
+
+@pytest.mark.parametrize("n_cell,n_cycle", [(500, 60), (3000, 120)])
+def test_synthetic_flat(n_cell, n_cycle):
+    from gtpower_b200 import synth
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=n_cell, n_cycle=n_cycle, seed=n_cell))
+    ev = synth.Trace(d, info, synth.TraceSpec(), seed=n_cycle).full()
+    res = run_engine(d, [ev])
+    compare(res, oracle(d, ev))
+
+
+def test_synthetic_skew_windows():
+    from gtpower_b200 import synth, windows
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=1500, n_cycle=80, seed=3))
+    ev = synth.Trace(d, info, synth.TraceSpec(mode=1, glitch_p=0.1), seed=9).full()
+    wins = windows.split(ev, d.ticks_per_cycle, [0, 17, 40, 41, 80])
+    res = run_engine(d, wins, cycles_per_tile=8)
+    compare(res, oracle(d, ev))
+
+
+def test_empty_trace():
+    d = toy.build([toy.inv_cell()], [(0, [0, 1]), (0, [-1, 2])], 3)
+    ev = toy.events(3, {})
+    res = run_engine(d, [ev])
+    compare(res, oracle(d, ev))
