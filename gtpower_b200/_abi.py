@@ -98,7 +98,7 @@ EXPORTED = [
     "gtp_config_default", "gtp_create", "gtp_destroy", "gtp_last_error", "gtp_n_period",
     "gtp_ticks_per_cycle", "gtp_reset", "gtp_push_events", "gtp_push_events_device",
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
-    "gtp_pack_values",
+    "gtp_evaluate_noalloc", "gtp_pack_values",
 ]
 
 _lib = None
@@ -145,6 +145,8 @@ def lib() -> C.CDLL:
     L.gtp_finalize.restype = C.c_int32
     L.gtp_fetch.argtypes = [C.c_void_p, _P, _P, _P, _P, C.POINTER(gtp_counts)]
     L.gtp_fetch.restype = C.c_int32
+    L.gtp_evaluate_noalloc.argtypes = [C.c_void_p, C.POINTER(gtp_events), _P, _P, _P]
+    L.gtp_evaluate_noalloc.restype = C.c_int32
     L.gtp_pack_values.argtypes = [_P, C.c_int64, _P]
     L.gtp_pack_values.restype = None
     _lib = L

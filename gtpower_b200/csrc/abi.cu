@@ -469,3 +469,130 @@ void gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free evaluation.
+//
+// Some callers cannot allocate device memory while they run: an EDA host
+// that embeds this engine under its own device-memory arena (reserved once at
+// start-up and shared with timing analysis), or a service whose latency
+// budget cannot absorb the device-wide synchronization cudaMalloc/cudaFree
+// can cause. For them gtp_evaluate_noalloc evaluates a whole trace with its
+// accumulators in the fixed static device array below instead of memory the
+// context allocates, and writes the results into device buffers the caller
+// provides. It calls no cudaMalloc, cudaFree or other allocating routine.
+//
+// The array is 16 MiB; every GPU that loads this library holds it until the
+// process exits. All calls share it and it keeps the last call's contents:
+// each call clears the part it uses before the walk, and two calls that
+// overlap on the GPU (different streams or contexts on one device) race.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the static array on the current device, looked up once
+// per device with that device current.
+cudaError_t noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  return cudaSuccess;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, float* d_cell5,
+                                           float* d_cycle5, double* d_totals) {
+  if (!c || !ev) return GTP_EINVAL;
+  if (ev->n_event < 0 || !ev->net_off || (ev->n_event > 0 && (!ev->time || !ev->value_packed))) {
+    c->err = "noalloc: missing event arrays";
+    return GTP_EINVAL;
+  }
+  if (ev->t_lo != 0 || ev->t_hi <= 0) {
+    c->err = "noalloc: evaluates a whole trace; t_lo must be 0 and t_hi > 0";
+    return GTP_EINVAL;
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: cudaGetDevice");
+  if (dev != c->device) {
+    c->err = "noalloc: the context's device must be current";
+    return GTP_EINVAL;
+  }
+  const Packed& P = c->P;
+  const size_t nc = static_cast<size_t>(std::max<int32_t>(1, P.n_cell));
+  const size_t ny = static_cast<size_t>(P.n_period + 1);
+  // layout: cell_acc | cyc_acc | tg | leak_tmp
+  const size_t off_cell = 0;
+  const size_t off_cyc = align256(off_cell + sizeof(double) * kNumCellAcc * nc);
+  const size_t off_tg = align256(off_cyc + sizeof(unsigned long long) * kNumCycAcc * ny);
+  const size_t off_tmp = align256(off_tg + sizeof(double) * (GTP_N_GROUP + 1) * 5);
+  const size_t need = align256(off_tmp + sizeof(unsigned long long) * ny);
+  if (need > kNoAllocScratchBytes) {
+    c->err = "noalloc: design needs " + std::to_string(need) + " bytes of scratch (40 per cell + 56 per "
+             "cycle); the static array holds " + std::to_string(kNoAllocScratchBytes);
+    return GTP_EOVERFLOW;
+  }
+  unsigned char* s = nullptr;
+  e = noalloc_scratch(dev, &s);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: cudaGetSymbolAddress");
+
+  // accumulators must start at zero
+  e = cudaMemsetAsync(s, 0, off_tg, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: clear");
+
+  KParams k = make_params(c);
+  k.cell_acc = reinterpret_cast<double*>(s + off_cell);
+  k.cyc_acc = reinterpret_cast<unsigned long long*>(s + off_cyc);
+  k.cnt_cell = nullptr;
+  k.cnt_cyc = nullptr;
+  k.net_off = ev->net_off;
+  k.ev_t = ev->time;
+  k.ev_v = ev->value_packed;
+  k.net_base = ev->net_base;
+  k.n_event = ev->n_event;
+  k.t_lo = 0;
+  k.t_hi = ev->t_hi;
+  const int64_t last_tick = std::min<int64_t>(ev->t_hi - 1, P.tmax);
+  k.cyc0 = 0;
+  const int64_t n_cyc = std::max<int64_t>(1, last_tick / P.tpc + 1);
+  int64_t ct = c->cfg.cycles_per_tile > 0 ? c->cfg.cycles_per_tile : 1024;
+  ct = std::min<int64_t>(ct, n_cyc);
+  ct = std::min<int64_t>(ct, 3072);
+  ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);
+  if (ct > 3072) { c->err = "noalloc: trace spans too many cycles for one launch"; return GTP_EOVERFLOW; }
+  k.cycles_per_tile = ct;
+  k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
+  const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+  k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
+  static const int bucket_pins[3] = {4, 8, kMaxPins};
+  for (int b = 0; b < 3; ++b) {
+    k.order_begin = P.bucket_begin[b];
+    k.order_end = P.bucket_begin[b + 1];
+    if (k.order_end <= k.order_begin) continue;
+    e = launch_power_walk(k, bucket_pins[b], false, threads, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: power walk launch");
+  }
+  double* tg = reinterpret_cast<double*>(s + off_tg);
+  e = launch_finalize(k, c->d_cell_group, d_cell5, d_cycle5, tg,
+                      reinterpret_cast<unsigned long long*>(s + off_tmp), c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: finalize");
+  if (d_totals) {
+    e = cudaMemcpyAsync(d_totals, tg, sizeof(double) * 5, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: totals");
+  }
+  return GTP_OK;
+}

@@ -271,6 +271,27 @@ gtp_status  gtp_finalize(gtp_ctx* ctx);
 gtp_status  gtp_fetch(gtp_ctx* ctx, float* cell5, float* cycle5,
                       double* totals, double* groups, gtp_counts* counts);
 
+/* Allocation-free evaluation. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they run, e.g. an
+ * EDA host that embeds the engine under its own device-memory arena reserved
+ * at start-up, or a service that cannot absorb the device-wide
+ * synchronization cudaMalloc/cudaFree may cause. It evaluates one whole
+ * trace (t_lo = 0) of device-resident events d_ev against the context's
+ * design and writes cell5 [n_cell][5], cycle5 [5][n_period] and totals [5]
+ * (layouts as gtp_fetch) into caller device buffers (d_totals may be NULL).
+ * It calls no cudaMalloc, cudaFree or other allocating routine: its
+ * accumulators live in a 16 MiB static device array that every GPU loading
+ * the library holds until exit. Limit: 40 bytes per cell + 56 per cycle
+ * within 16 MiB (about 300k cells x 20k cycles); larger designs get
+ * GTP_EOVERFLOW. The first call on a device looks up the array's address;
+ * make that first call before any stream capture. All calls share the array
+ * (each clears what it uses first), so calls that overlap on the GPU race.
+ * Work is queued on the context's stream; gtp_sync waits and reports
+ * invalid events. */
+gtp_status  gtp_evaluate_noalloc(gtp_ctx* ctx, const gtp_events* d_ev, float* d_cell5,
+                                 float* d_cycle5, double* d_totals);
+
 /* Packs one value per byte (0..3) into the 2-bit layout of value_packed. */
 void        gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed);
 
