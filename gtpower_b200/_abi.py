@@ -84,7 +84,8 @@ class gtp_config(C.Structure):
     _fields_ = [("cuda_device_id", C.c_int32), ("cycles_per_tile", C.c_int32),
                 ("n_thread_per_block", C.c_int32), ("gates_per_block", C.c_int32),
                 ("max_n_pin_for_leakage_power", C.c_int32), ("collect_counts", C.c_int32),
-                ("max_event_num", C.c_int64), ("reserved", C.c_int64 * 4)]
+                ("max_event_num", C.c_int64), ("sort_by_work", C.c_int32),
+                ("reserved32", C.c_int32), ("reserved", C.c_int64 * 3)]
 
 
 class gtp_counts(C.Structure):

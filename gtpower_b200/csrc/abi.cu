@@ -33,6 +33,13 @@ struct gtp_ctx {
   DevType* d_types = nullptr;
   DevSlot* d_slots = nullptr;
   uint2* d_cubes = nullptr;
+  int32_t* d_type_fast_off = nullptr;
+  int16_t* d_fast_tab = nullptr;
+  // per-window walk order sorted by work
+  unsigned long long *d_keys_in = nullptr, *d_keys_out = nullptr;
+  int32_t* d_order_work = nullptr;
+  void* d_sort_temp = nullptr;
+  size_t sort_temp_bytes = 0;
   // events (host-pushed windows)
   int64_t ev_cap = 0, net_cap_set = 0;
   int64_t *d_net_off = nullptr, *d_ev_t = nullptr, *d_net_base = nullptr;
@@ -86,7 +93,8 @@ void free_all(gtp_ctx* c) {
                   c->d_leak_pool, c->d_inst, c->d_types, c->d_slots, c->d_cubes, c->d_net_off,
                   c->d_ev_t, c->d_net_base, c->d_ev_v, c->d_cell_acc, c->d_cyc_acc,
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
-                  c->d_leak_tmp};
+                  c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
+                  c->d_keys_out, c->d_order_work, c->d_sort_temp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -110,6 +118,14 @@ KParams make_params(gtp_ctx* c) {
   k.cubes = c->d_cubes;
   k.leak_pool = c->d_leak_pool;
   k.inst = c->d_inst;
+  k.type_fast_off = c->d_type_fast_off;
+  k.fast_tab = c->d_fast_tab;
+  k.drift = P.drift ? 1 : 0;
+  k.n_fast_tab = static_cast<int32_t>(P.fast_tab.size());
+  k.n_leak_pool = static_cast<int32_t>(P.leak_pool.size());
+  k.tabs_in_smem = (P.fast_tab.size() * 2 + P.leak_pool.size() * 4) <= 16384 ? 1 : 0;
+  k.fast_inst_stride = P.fast_inst_floats + 1;   // odd stride: no shared-memory bank conflicts
+  k.tmax_s = static_cast<double>(P.tmax) * P.ts;
   k.n_net = P.n_net;
   k.tpc = P.tpc;
   k.inv_tpc = 1.0 / static_cast<double>(P.tpc);
@@ -128,6 +144,13 @@ KParams make_params(gtp_ctx* c) {
   k.n_cell = P.n_cell;
   k.status = c->d_status;
   return k;
+}
+
+// Largest cycle tile whose shared memory (bins with counters, event
+// buffers, tables) stays within 227 KB.
+int64_t max_cycles_per_tile(int threads) {
+  const int64_t budget = 227 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4));
+  return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (kNumCycAcc * 8 + 8)));
 }
 
 gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
@@ -158,17 +181,28 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   const int64_t cyc_end = last_tick / P.tpc + 1;
   const int64_t n_cyc = std::max<int64_t>(1, cyc_end - k.cyc0);
   int64_t ct = c->cfg.cycles_per_tile;
-  if (ct <= 0) ct = 1024;
+  if (ct <= 0) ct = 512;
   ct = std::min<int64_t>(ct, n_cyc);
-  const int64_t max_ct = 3072;  // keeps the bins within 227 KB of shared memory
+  const int threads_ = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+  // bins + event buffers + tables within 227 KB of shared memory; tile span
+  // (ct+1)*tpc within 2^31 ticks, as the walk holds times as 32-bit offsets
+  // from the tile start
+  const int64_t max_ct = std::min<int64_t>(max_cycles_per_tile(threads_), (int64_t(INT32_MAX) / P.tpc) - 1);
   ct = std::min(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);  // grid.y limit
-  if (ct > max_ct) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
+  if (ct > max_ct || ct < 1) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
   k.cycles_per_tile = ct;
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
   const bool counts = c->cfg.collect_counts != 0;
+  if (c->cfg.sort_by_work && c->d_order_work) {
+    cudaError_t e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in,
+                                       c->d_keys_out, c->d_order_work, c->d_sort_temp,
+                                       c->sort_temp_bytes, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
+    k.order = c->d_order_work;
+  }
   static const int bucket_pins[3] = {4, 8, kMaxPins};
   for (int b = 0; b < 3; ++b) {
     k.order_begin = P.bucket_begin[b];
@@ -213,6 +247,7 @@ void gtp_config_default(gtp_config* cfg) {
   cfg->max_n_pin_for_leakage_power = 16;
   cfg->collect_counts = 0;
   cfg->max_event_num = 0;  // 0 = no cap other than device memory
+  cfg->sort_by_work = 1;
 }
 
 gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ctx** out) {
@@ -260,6 +295,8 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
   UP(d_types, P.types);
   UP(d_slots, P.slots);
   UP(d_cubes, cubes);
+  UP(d_type_fast_off, P.type_fast_off);
+  UP(d_fast_tab, P.fast_tab);
 #undef UP
   {
     const size_t nc = std::max<int32_t>(1, P.n_cell);
@@ -273,6 +310,13 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     if (e == cudaSuccess) e = cudaMalloc(&c->d_cycle5, sizeof(float) * 5 * ny);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_tg, sizeof(double) * (GTP_N_GROUP + 1) * 5);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_leak_tmp, sizeof(unsigned long long) * ny);
+    if (e == cudaSuccess && c->cfg.sort_by_work && P.n_cell > 0) {
+      c->sort_temp_bytes = std::max<size_t>(1, work_sort_temp_bytes(P.n_cell));
+      e = cudaMalloc(&c->d_keys_in, sizeof(unsigned long long) * nc);
+      if (e == cudaSuccess) e = cudaMalloc(&c->d_keys_out, sizeof(unsigned long long) * nc);
+      if (e == cudaSuccess) e = cudaMalloc(&c->d_order_work, sizeof(int32_t) * nc);
+      if (e == cudaSuccess) e = cudaMalloc(&c->d_sort_temp, c->sort_temp_bytes);
+    }
     if (e != cudaSuccess) goto cuda_err;
   }
   // fixed-point scales: dynamic energies bounded by max|E| * 2^36 events,
@@ -569,11 +613,14 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   const int64_t last_tick = std::min<int64_t>(ev->t_hi - 1, P.tmax);
   k.cyc0 = 0;
   const int64_t n_cyc = std::max<int64_t>(1, last_tick / P.tpc + 1);
-  int64_t ct = c->cfg.cycles_per_tile > 0 ? c->cfg.cycles_per_tile : 1024;
+  int64_t ct = c->cfg.cycles_per_tile > 0 ? c->cfg.cycles_per_tile : 512;
   ct = std::min<int64_t>(ct, n_cyc);
-  ct = std::min<int64_t>(ct, 3072);
+  const int64_t max_ct = std::min<int64_t>(
+      max_cycles_per_tile(c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256),
+      (int64_t(INT32_MAX) / P.tpc) - 1);
+  ct = std::min<int64_t>(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);
-  if (ct > 3072) { c->err = "noalloc: trace spans too many cycles for one launch"; return GTP_EOVERFLOW; }
+  if (ct > max_ct || ct < 1) { c->err = "noalloc: trace spans too many cycles for one launch"; return GTP_EOVERFLOW; }
   k.cycles_per_tile = ct;
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;

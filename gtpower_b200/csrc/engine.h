@@ -62,6 +62,7 @@ struct DevSlot {
 };
 
 constexpr int kMaxPins = 32;      // cell pins supported by the walk
+constexpr int kFastPins = 4;      // cells up to this many pins use fast_tab
 constexpr int kNumCycAcc = 6;     // per-cycle fixed-point accumulators
 constexpr int kNumCellAcc = 5;
 
@@ -85,6 +86,17 @@ struct Packed {
   std::vector<uint32_t> cubes;   // pairs
   std::vector<float>   leak_pool;
   std::vector<float>   inst;
+  // per cell type with n_pin <= kFastPins: offset into fast_tab, else -1.
+  // fast_tab (int16): for input pin i, [i][ones] = energy offset of the
+  // first internal_power group whose `when` holds in pin state `ones` (-1 =
+  // none); then for output o and related input q, [o][q][ones] likewise.
+  std::vector<int32_t> type_fast_off;
+  std::vector<int16_t> fast_tab;
+  // true when some tick lies between a cycle's tick boundary and its
+  // seconds boundary (c*clk_period), where the reference's per-cycle
+  // leakage split departs from the plain overlap (needs the drift path)
+  bool drift = false;
+  int32_t fast_inst_floats = 0;   // largest instance block of a fast cell type
   // bucket ranges in order[]: cells with n_pin <= 4, <= 8, <= 32
   int32_t bucket_begin[4] = {0, 0, 0, 0};
   double max_abs_energy = 0;     // max |instance energy|, for the fixed-point scale
@@ -111,6 +123,12 @@ struct KParams {
   const uint2* cubes;
   const float* leak_pool;
   const float* inst;
+  const int32_t* type_fast_off;
+  const int16_t* fast_tab;
+  int32_t n_fast_tab, n_leak_pool;  // table sizes (for staging in shared memory)
+  int32_t tabs_in_smem;
+  int32_t fast_inst_stride;         // floats per thread for a staged instance block
+  int32_t drift;
   // events
   const int64_t* net_off;
   const int64_t* ev_t;
@@ -128,6 +146,7 @@ struct KParams {
   int64_t tmax;
   int64_t n_period;
   float min_diff0;           // float(time_max * timescale)
+  double tmax_s;             // time_max * timescale (s)
   // tiling
   int64_t cyc0;              // first cycle of the window
   int64_t cycles_per_tile;
@@ -154,7 +173,16 @@ constexpr int32_t kErrContext = 8;
 // Launches the walk over one bucket of cells. shared-memory bytes computed inside.
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
                               cudaStream_t stream);
-size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts);
+size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
+                             size_t tab_bytes);
+
+// Walk order for one window: cells stay grouped by pin bucket and, within a
+// bucket, are sorted by the number of events on their pins (descending).
+size_t work_sort_temp_bytes(int32_t n_cell);
+cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int32_t n_cell,
+                               const int32_t* bucket_begin, unsigned long long* keys_in,
+                               unsigned long long* keys_out, int32_t* order_out, void* temp,
+                               size_t temp_bytes, cudaStream_t stream);
 
 // Finalize kernels: per-cell floats, totals/groups, per-cycle floats.
 cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,

@@ -196,6 +196,7 @@ gtp_status pack_design(const gtp_design& d, int max_leak_pins, Packed& P, std::s
     e += 2 * n_out;
     dt.delay_off = e;
     e += 4 * n_out * ty.n_in;
+    e = (e + 3) & ~3;   // 16-byte aligned blocks (staged with vector loads)
     dt.inst_floats = e;
 
     // leakage (Power::getLeakagePower)
@@ -354,6 +355,56 @@ gtp_status pack_design(const gtp_design& d, int max_leak_pins, Packed& P, std::s
     for (auto& x : th) x.join();
   }
   for (double v : max_e) P.max_abs_energy = std::max(P.max_abs_energy, v);
+
+  // ---- fast tables: first matching group per (pin, related, state) ----
+  P.type_fast_off.assign(d.n_type, -1);
+  for (int32_t t = 0; t < d.n_type; ++t) {
+    const DevType& dt = P.types[t];
+    if (dt.n_pin > kFastPins) continue;
+    const int n_state = 1 << dt.n_pin;
+    const int n_in = dt.n_in, n_out = dt.n_pin - dt.n_in;
+    P.type_fast_off[t] = static_cast<int32_t>(P.fast_tab.size());
+    auto holds = [&](const DevSlot& sl, uint32_t ones) {
+      for (int k = 0; k < sl.n_cube; ++k) {
+        const uint32_t care = P.cubes[2 * (sl.cube_off + k)];
+        const uint32_t val = P.cubes[2 * (sl.cube_off + k) + 1];
+        if ((ones & care) == val) return true;
+      }
+      return false;
+    };
+    for (int pin = 0; pin < n_in; ++pin)
+      for (int s = 0; s < n_state; ++s) {
+        int16_t e = -1;
+        for (int32_t k = P.pin_slot[dt.pin_slot_off + pin]; k < P.pin_slot[dt.pin_slot_off + pin + 1]; ++k)
+          if (holds(P.slots[k], static_cast<uint32_t>(s))) { e = static_cast<int16_t>(P.slots[k].e_off); break; }
+        P.fast_tab.push_back(e);
+      }
+    for (int o = 0; o < n_out; ++o)
+      for (int q = 0; q < n_in; ++q)
+        for (int s = 0; s < n_state; ++s) {
+          int16_t e = -1;
+          const int pin = n_in + o;
+          for (int32_t k = P.pin_slot[dt.pin_slot_off + pin]; k < P.pin_slot[dt.pin_slot_off + pin + 1]; ++k) {
+            if (P.slots[k].related != q) continue;
+            if (holds(P.slots[k], static_cast<uint32_t>(s))) { e = static_cast<int16_t>(P.slots[k].e_off); break; }
+          }
+          P.fast_tab.push_back(e);
+        }
+    if (dt.inst_floats > INT16_MAX) return fail("instance block too large for the fast tables");
+    P.fast_inst_floats = std::max(P.fast_inst_floats, dt.inst_floats);
+  }
+
+  // ---- clock drift: does some tick fall between a cycle's tick boundary
+  // c*tpc and its seconds boundary c*period (double comparisons as the
+  // reference's calculatePerCycleLeakagePower makes them)? ----
+  P.drift = false;
+  for (int64_t c = 1; c <= P.n_period + 1 && !P.drift; ++c) {
+    const double b = static_cast<double>(c) * P.period_d;
+    const int64_t t0 = c * P.tpc;
+    const bool at = b <= static_cast<double>(t0) * P.ts;
+    const bool before = b <= static_cast<double>(t0 - 1) * P.ts;
+    if (!at || before) P.drift = true;
+  }
 
   // ---- walk order: bucket by pin count (register footprint), then by type ----
   P.order.resize(d.n_cell);

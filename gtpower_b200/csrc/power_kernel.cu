@@ -3,38 +3,57 @@
 // One thread walks one cell over one cycle tile of the event window. It
 // merges the cell's pin event lists in time order (the loop of
 // findTimeBasedAllPower, power/TimeBasedPower.cc:795-890) and, per step:
-//   - charges the leakage of the state before the step over the elapsed
-//     segment, split into clock cycles exactly as
-//     calculatePerCycleLeakagePower does (TimeBasedPower.cc:677-701);
-//   - classifies each triggered pin's event as glitch or not with the
-//     clock-period grouping of getEventClockCycleBasedGlitchFlags
-//     (TimeBasedPower.cc:589-637), evaluated online from the neighbouring
-//     events, and scales it with getTimeBasedGlitchScalingRatioH
-//     (power/PowerUtils.cc:285-294);
-//   - selects the input internal energy (first `when`-matching group) or,
-//     for an output event, the related input pin by arc-delay distance
-//     (TimeBasedPower.cc:383-509) and its energy, plus C*V^2 switching.
+//   - leakage: the cell's leakage changes only when its pin state changes.
+//     Each change adds its difference to a per-cycle level (a run-difference
+//     array, prefix-summed at finalize) and its share of its own cycle, so
+//     the per-cycle integral of the state-dependent leakage — what
+//     calculatePerCycleLeakagePower (TimeBasedPower.cc:677-701) computes
+//     segment by segment — costs O(1) per state change and nothing per
+//     idle cycle. Where a tick falls between a cycle's tick boundary and its
+//     seconds boundary (c*clk_period), the reference's split departs from
+//     the plain overlap; the drift path adds exactly those differences;
+//   - glitch: the clock-period grouping of getEventClockCycleBasedGlitchFlags
+//     (TimeBasedPower.cc:589-637); an event is isolated in its period unless
+//     its neighbours say otherwise (two compares from registers), and only
+//     then is the period scanned;
+//   - internal energy: the first `when`-matching internal_power group
+//     (findInputInternalVal, TimeBasedPower.cc:341-381) — for cells of up to
+//     four pins a table lookup by pin state; for an output event, the
+//     related input by arc-delay distance from the per-pin last-event
+//     registers (findOutputInternalVal, TimeBasedPower.cc:383-509); plus
+//     C*V^2 switching per rise.
 //
-// Design for B200:
-//   - the CTA owns a cycle tile; per-cycle sums go to shared-memory bins as
-//     64-bit fixed-point energies (integer shared atomics: exact, and the
-//     final per-cycle values do not depend on accumulation order). Leakage of
-//     whole idle cycles is added as a run (+x at the first full cycle, -x
-//     after the last) so an idle stretch costs O(1), not O(cycles);
-//   - a tile flushes its bins to global memory once;
-//   - per-cell sums stay in FP64 registers and are flushed once per tile;
-//   - a leakage segment is charged by the tile in which it starts, so a
-//     segment that crosses a tile edge is split exactly as the reference
-//     splits it (no artificial cut).
+// Per-cycle sums go to shared-memory bins as 64-bit fixed-point energies
+// (integer shared atomics: exact, and the per-cycle outputs do not depend on
+// accumulation order); a tile flushes its bins once. Per-cell sums stay in
+// FP64 registers and are flushed once per tile. Event times are held as
+// 32-bit offsets from the tile start.
 #include <cstdint>
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include "engine.h"
 
+#ifndef WALK_MIN_BLOCKS
+#define WALK_MIN_BLOCKS 2   // 2 x 256 threads per SM keeps the walk spill-free
+#endif
+
 namespace gtpb {
 namespace {
 
-constexpr int64_t kInf = INT64_MAX;
+constexpr uint32_t kRelInf = 0xFFFFFFFFu;     // no further event
+constexpr uint32_t kRelBeyond = 0xFFFFFFFEu;  // next event at or after the tile end
+constexpr int32_t kFarBefore = INT32_MIN / 2;
+#ifndef WALK_RING
+#define WALK_RING 8
+#endif
+#ifndef WALK_USE_RING
+#define WALK_USE_RING 0
+#endif
+#ifndef WALK_STAGE_INST
+#define WALK_STAGE_INST 1
+#endif
+constexpr int kRing = WALK_RING;               // events buffered per pin (RING path)
 
 __device__ __forceinline__ int64_t div_floor_pos(int64_t t, int64_t d, double inv) {
   // floor(t / d) for 0 <= t < 2^53 via a double reciprocal and one correction
@@ -53,10 +72,8 @@ __device__ __forceinline__ int64_t ev_time(const int64_t* __restrict__ t, int64_
   return __ldg(t + i);
 }
 
-// getNRise (power/PowerUtils.cc:213-237) as a 4x4 table packed in bits:
-// returns 2*n_rise (0, 1 or 2).
+// getNRise (power/PowerUtils.cc:213-237): returns 2*n_rise (0, 1 or 2).
 __device__ __forceinline__ int nrise2(int prev, int cur) {
-  // prev=0: cur 1 -> 2, cur 2 -> 1 ; prev=2: cur 1 -> 1 ; else 0
   if (prev == cur) return 0;
   if (cur == 1) return prev == 0 ? 2 : (prev == 2 ? 1 : 0);
   if (cur == 2) return prev == 0 ? 1 : 0;
@@ -81,73 +98,62 @@ __device__ __forceinline__ unsigned long long to_fx(double x, double s) {
   return static_cast<unsigned long long>(__double2ll_rn(x * s));
 }
 
+// Reads element i of a register array without dynamic indexing.
+template <int N, typename T>
+__device__ __forceinline__ T sel(const T (&a)[N], int i) {
+  T r = a[0];
+#pragma unroll
+  for (int j = 1; j < N; ++j)
+    if (j == i) r = a[j];
+  return r;
+}
+
 struct Bins {
-  unsigned long long* s;   // [6][ct]
+  unsigned long long* s;   // [6][ct] fixed-point energies
   uint32_t* sc;            // [2][ct] counts
   int64_t c_lo;            // first cycle of the tile
   int64_t ct;              // cycles in the tile
 };
 
-template <bool COUNTS>
-struct Walker {
-  const KParams& p;
-  Bins& b;
-  __device__ Walker(const KParams& pp, Bins& bb) : p(pp), b(bb) {}
+// per-cycle accumulator slots
+constexpr int kLeakPart = 0;   // leakage inside the cycle of each change
+constexpr int kLeakLevel = 1;  // run-difference of the per-cycle leakage level
+constexpr int kInt = 2, kGInt = 3, kSw = 4, kGSw = 5;
 
-  __device__ __forceinline__ void add_cyc(int q, int64_t c, double joules, double scale) {
-    if (joules == 0.0) return;
-    const unsigned long long x = to_fx(joules, scale);
-    const int64_t k = c - b.c_lo;
-    if (k >= 0 && k < b.ct) {
-      atomicAdd(b.s + q * b.ct + k, x);
-    } else {
-      const int64_t cc = c < p.n_period ? c : p.n_period;
-      atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
-    }
+__device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, int64_t c,
+                                        unsigned long long x) {
+  if (x == 0ull) return;
+  const int64_t k = c - b.c_lo;
+  if (k >= 0 && k < b.ct) {
+    atomicAdd(b.s + q * b.ct + k, x);
+  } else {
+    const int64_t cc = c < 0 ? p.n_period : (c < p.n_period ? c : p.n_period);
+    atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
   }
-  __device__ __forceinline__ void add_cnt(int q, int64_t c) {
-    const int64_t k = c - b.c_lo;
-    if (k >= 0 && k < b.ct) {
-      atomicAdd(b.sc + q * b.ct + k, 1u);
-    } else {
-      const int64_t cc = c < p.n_period ? c : p.n_period;
-      atomicAdd(p.cnt_cyc + q * (p.n_period + 1) + cc, 1ull);
-    }
-  }
+}
 
-  // calculatePerCycleLeakagePower over [prev, cur) ticks with value val (W).
-  __device__ void leak_segment(int64_t prev, int64_t cur, float val) {
-    if (val == 0.0f) return;
-    const double P = p.period_d;
-    const double cur_s = static_cast<double>(cur) * p.ts;
-    const double left = static_cast<double>(prev) * p.ts;
-    const int64_t c = div_floor_pos(prev, p.tpc, p.inv_tpc);
-    if (!(static_cast<double>(c) * P <= cur_s)) return;
-    const double r1 = static_cast<double>(c + 1) * P;
-    const double v = static_cast<double>(val);
-    if (!(r1 <= cur_s)) {
-      add_cyc(0, c, v * (cur_s - left), p.fx_leak);
-      return;
-    }
-    add_cyc(0, c, v * (r1 - left), p.fx_leak);
-    // last cycle k with k*P <= cur_s; (c+1)*P <= cur_s holds, so k >= c+1.
-    // The reciprocal estimate is within one or two of k, so both loops are short.
-    int64_t k = static_cast<int64_t>(cur_s * p.inv_period_d);
-    if (k < c + 1) k = c + 1;
-    while (k > c + 1 && static_cast<double>(k) * P > cur_s) --k;
-    while (static_cast<double>(k + 1) * P <= cur_s) ++k;
-    if (k >= c + 2) {
-      const double full = v * P;
-      add_cyc(1, c + 1, full, p.fx_leak);
-      add_cyc(1, k, -full, p.fx_leak);
-    }
-    if (k >= c + 1) add_cyc(0, k, v * (cur_s - static_cast<double>(k) * P), p.fx_leak);
+__device__ __forceinline__ void add_cnt(const KParams& p, const Bins& b, int q, int64_t c) {
+  const int64_t k = c - b.c_lo;
+  if (k >= 0 && k < b.ct) {
+    atomicAdd(b.sc + q * b.ct + k, 1u);
+  } else {
+    const int64_t cc = c < p.n_period ? c : p.n_period;
+    atomicAdd(p.cnt_cyc + q * (p.n_period + 1) + cc, 1ull);
   }
-};
+}
 
-// Period-group facts of event i on a net with accessible range [lo, hi) and
-// global index 0 at g0 (or -1): the first index of its clock period (never
-// g0) and the count k of non-initial events in the period.
+// Seconds cycle of tick t: the largest c with c*period <= t*ts (the
+// comparison calculatePerCycleLeakagePower's loop makes), given the tick
+// cycle c0 of t.
+__device__ __forceinline__ int64_t seconds_cycle(const KParams& p, int64_t t, int64_t c0) {
+  const double ts = static_cast<double>(t) * p.ts;
+  int64_t s = c0;
+  while (s > 0 && !(static_cast<double>(s) * p.period_d <= ts)) --s;
+  while (static_cast<double>(s + 1) * p.period_d <= ts) ++s;
+  return s;
+}
+
+// Period-group bounds of event i (global index 0 at g0 never counts).
 struct Group {
   int64_t first;
   int64_t last;
@@ -165,19 +171,55 @@ __device__ __forceinline__ Group period_group(const int64_t* __restrict__ t, int
   return g;
 }
 
-// Reads element i of a register array without dynamic indexing (keeps the
-// array in registers).
-template <int N>
-__device__ __forceinline__ int64_t sel(const int64_t (&a)[N], int i) {
-  int64_t r = a[0];
-#pragma unroll
-  for (int j = 1; j < N; ++j)
-    if (j == i) r = a[j];
-  return r;
+// Glitch scaling ratio of event e on a net (getGlitchScalingRatioClockCycleBasedH
+// and getTimeBasedGlitchScalingRatioH, TimeBasedPower.cc:303-339,
+// PowerUtils.cc:285-294); -1 when the event is not a glitch event.
+__device__ float glitch_ratio(const KParams& p, int64_t e, int64_t lo, int64_t hi, int64_t g0,
+                              int64_t cur, int64_t cyc_start, float den) {
+  if (e == g0) return -1.0f;
+  const Group gr = period_group(p.ev_t, e, lo, hi, g0, cyc_start, cyc_start + p.tpc);
+  const int64_t k = gr.last - gr.first + 1;
+  const int64_t lim = k >= 2 ? (k & ~int64_t(1)) : 0;
+  if (!(e - gr.first < lim)) return -1.0f;
+  int64_t w = -1;
+  if (e - 1 >= lo) {
+    bool pflag;
+    if (e - 1 >= gr.first) {
+      pflag = true;
+    } else if (e - 1 == g0) {
+      pflag = false;
+    } else {
+      const int64_t tp = ev_time(p.ev_t, e - 1);
+      const int64_t pc = div_floor_pos(tp, p.tpc, p.inv_tpc);
+      const Group gp = period_group(p.ev_t, e - 1, lo, hi, g0, pc * p.tpc, pc * p.tpc + p.tpc);
+      const int64_t kp = gp.last - gp.first + 1;   // e-1 is the last of its period
+      pflag = kp >= 2 && (kp & 1) == 0;
+    }
+    if (pflag) w = cur - ev_time(p.ev_t, e - 1);
+  }
+  if (e + 1 < hi) {
+    bool nflag;
+    const int64_t tn = ev_time(p.ev_t, e + 1);
+    if (e + 1 <= gr.last) {
+      nflag = (e + 1 - gr.first) < lim;
+    } else if (e + 2 < hi) {
+      const int64_t nc = div_floor_pos(tn, p.tpc, p.inv_tpc);
+      nflag = ev_time(p.ev_t, e + 2) < nc * p.tpc + p.tpc;
+    } else {
+      nflag = false;
+    }
+    if (nflag) w = max(w, tn - cur);
+  }
+  if (w < 0) return -1.0f;
+  if (den == 0.0f) return 1.0f;
+  const float pw = __double2float_rn(__dmul_rn(static_cast<double>(w), p.ts));
+  const float r = __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(pw), 2.0),
+                                              static_cast<double>(den)));
+  return fminf(1.0f, __fmul_rn(r, r));
 }
 
-template <int MAXP, bool COUNTS>
-__global__ void __launch_bounds__(256) power_walk_kernel(const KParams p) {
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+__global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const KParams p) {
   extern __shared__ unsigned long long smem[];
   const int64_t ct = p.cycles_per_tile;
   Bins bins;
@@ -189,258 +231,394 @@ __global__ void __launch_bounds__(256) power_walk_kernel(const KParams p) {
   for (int64_t k = threadIdx.x; k < kNumCycAcc * ct; k += blockDim.x) smem[k] = 0ull;
   if (COUNTS)
     for (int64_t k = threadIdx.x; k < 2 * ct; k += blockDim.x) bins.sc[k] = 0u;
+  // RING: per-thread event buffers [pin][slot][thread] of times - T0, then
+  // the per-type energy-selection and leakage tables when they fit
+  constexpr bool RING = FAST && WALK_USE_RING;
+  constexpr bool STAGE = FAST && WALK_STAGE_INST;
+  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + kNumCycAcc * ct + (COUNTS ? ct : 0));
+  const int nt_blk = blockDim.x;
+  const int16_t* fast_tab = p.fast_tab;
+  const float* leak_pool = p.leak_pool;
+  float* s_tabs = reinterpret_cast<float*>(ring + (RING ? MAXP * kRing * nt_blk : 0));
+  if (FAST && p.tabs_in_smem) {
+    float* s_leak = s_tabs;
+    int16_t* s_fast = reinterpret_cast<int16_t*>(s_leak + p.n_leak_pool);
+    for (int k = threadIdx.x; k < p.n_leak_pool; k += blockDim.x) s_leak[k] = __ldg(p.leak_pool + k);
+    for (int k = threadIdx.x; k < p.n_fast_tab; k += blockDim.x) s_fast[k] = __ldg(p.fast_tab + k);
+    leak_pool = s_leak;
+    fast_tab = s_fast;
+  }
+  // STAGE: each thread's copy of its cell's instance block (energies, delays)
+  float* s_inst = s_tabs + (FAST && p.tabs_in_smem ? ((p.n_leak_pool * 4 + p.n_fast_tab * 2 + 15) / 16) * 4 : 0)
+                  + threadIdx.x * p.fast_inst_stride;
   __syncthreads();
 
-  // tile window in ticks
+  // tile window in ticks: [T0, T0 + span)
   const int64_t T0 = max(p.t_lo, bins.c_lo * p.tpc);
   const bool last_tile = (tile == p.n_tiles - 1);
-  const int64_t T1 = last_tile ? p.t_hi : min(p.t_hi, (bins.c_lo + ct) * p.tpc);
+  const int64_t T1 = last_tile ? min(p.t_hi, p.tmax + 1) : min(p.t_hi, (bins.c_lo + ct) * p.tpc);
+  const uint32_t span = static_cast<uint32_t>(T1 > T0 ? T1 - T0 : 0);
   const bool owns_initial = (tile == 0) && (p.t_lo == 0);
+  const double P = p.period_d;
 
-  Walker<COUNTS> W(p, bins);
   const int32_t g_begin = p.order_begin + blockIdx.x * p.gates_per_block;
   const int32_t g_end = min(p.order_end, g_begin + p.gates_per_block);
 
   for (int32_t gi = g_begin + threadIdx.x; gi < g_end; gi += blockDim.x) {
     const int32_t cell = __ldg(p.order + gi);
     const int32_t p0 = __ldg(p.cell_pin_off + cell);
-    const DevType ty = p.types[__ldg(p.cell_type + cell)];
-    const float* __restrict__ blk = p.inst + __ldg(p.cell_inst + cell);
+    const int32_t type = __ldg(p.cell_type + cell);
+    const DevType ty = p.types[type];
+    const float* __restrict__ blk_g = p.inst + __ldg(p.cell_inst + cell);
     const int n_pin = ty.n_pin, n_in = ty.n_in;
+    const int n_state = 1 << (n_pin < 16 ? n_pin : 0);
+    const int32_t fo = FAST ? __ldg(p.type_fast_off + type) : 0;
+    if (STAGE) {
+      // blocks are padded to a multiple of 4 floats and 16-byte aligned
+      const float4* src = reinterpret_cast<const float4*>(blk_g);
+      for (int k = 0; k < ty.inst_floats / 4; ++k) {
+        const float4 v = __ldg(src + k);
+        s_inst[4 * k + 0] = v.x; s_inst[4 * k + 1] = v.y; s_inst[4 * k + 2] = v.z; s_inst[4 * k + 3] = v.w;
+      }
+    }
+    const float* blk = STAGE ? s_inst : blk_g;
 
-    int64_t f[MAXP], hi[MAXP], lo[MAXP], nt[MAXP], g0[MAXP];
-    uint64_t state = 0;     // 2 bits per pin
-    uint32_t ones = 0;      // bit per pin: state == 1
-    uint32_t has_wave = 0;
+    int64_t f[MAXP];          // next event index to read (absolute)
+    int32_t rem[MAXP];        // events left to read in the accessible range
+    uint32_t rs[MAXP];        // RING: head slot | (events held << 8)
+    uint32_t rv[MAXP];        // RING: 2-bit values of the held events by slot
+    uint32_t nt[MAXP];        // next event time - T0, or kRelBeyond / kRelInf
+    int32_t lt[MAXP];         // time of the last event strictly before now - T0
+    uint32_t state = 0;       // 2 bits per pin (MAXP <= 16) ...
+    uint64_t state_hi = 0;    // ... pins 16..31
+    uint32_t ones = 0;        // bit per pin: state == 1
+    uint32_t nvals = 0;       // prefetched value of each pin's next event (pins < 16)
+    uint64_t nvals_hi = 0;
+    uint32_t has_wave = 0, clock_mask = 0, at_lo = 0, last_rise = 0;
+    auto get_v = [&](uint32_t s_lo, uint64_t s_hi, int i) -> int {
+      return i < 16 ? static_cast<int>((s_lo >> (2 * i)) & 3) : static_cast<int>((s_hi >> (2 * (i - 16))) & 3);
+    };
+    auto set_v = [&](uint32_t& s_lo, uint64_t& s_hi, int i, int v) {
+      if (i < 16) s_lo = (s_lo & ~(3u << (2 * i))) | (static_cast<uint32_t>(v) << (2 * i));
+      else s_hi = (s_hi & ~(3ull << (2 * (i - 16)))) | (static_cast<uint64_t>(v) << (2 * (i - 16)));
+    };
+    auto rel = [&](int64_t t) -> uint32_t {
+      const int64_t r = t - T0;
+      return (r >= 0 && r < static_cast<int64_t>(span)) ? static_cast<uint32_t>(r) : kRelBeyond;
+    };
+    // RING: read up to kRing events of pin i into its buffer with
+    // independent loads (one memory latency per kRing events)
+    auto refill = [&](int i) {
+      const int32_t rem_i = sel<MAXP>(rem, i);
+      const int n = rem_i < kRing ? rem_i : kRing;
+      const int64_t a = sel<MAXP>(f, i);
+      const int64_t w0 = a >> 4;
+      const uint32_t vw0 = __ldg(p.ev_v + w0);
+      const uint32_t vw1 = ((a + n - 1) >> 4) != w0 ? __ldg(p.ev_v + w0 + 1) : 0u;
+      uint32_t vals = 0;
+#pragma unroll 4
+      for (int j = 0; j < n; ++j) {
+        {
+          const int64_t idx = a + j;
+          const int64_t tj = ev_time(p.ev_t, idx);
+          if (tj > p.tmax) atomicOr(p.status, kErrTimeRange);
+          ring[(i * kRing + j) * nt_blk + threadIdx.x] = rel(tj);
+          const uint32_t w = (idx >> 4) == w0 ? vw0 : vw1;
+          vals |= ((w >> (2 * (idx & 15))) & 3u) << (2 * j);
+        }
+      }
+      const uint32_t head = ring[(i * kRing) * nt_blk + threadIdx.x];
+#pragma unroll
+      for (int j = 0; j < MAXP; ++j) {
+        if (j == i) {
+          rv[j] = vals;
+          rs[j] = static_cast<uint32_t>(n) << 8;
+          f[j] = a + n;
+          rem[j] = rem_i - n;
+          nt[j] = head;
+        }
+      }
+    };
+    // pins whose buffer must be (re)filled before the next merge step
+    uint32_t need = 0;
+    auto do_refills = [&](int64_t after) {
+      while (need) {
+        const int i = __ffs(need) - 1;
+        need &= need - 1;
+        refill(i);
+        const uint32_t h = sel<MAXP>(nt, i);
+        if (static_cast<int64_t>(h) <= after) atomicOr(p.status, kErrTimeOrder);
+      }
+    };
 #pragma unroll
     for (int i = 0; i < MAXP; ++i) {
-      f[i] = 0; hi[i] = 0; lo[i] = 0; nt[i] = kInf; g0[i] = -1;
+      f[i] = 0; rem[i] = 0; nt[i] = kRelInf; lt[i] = kFarBefore; rs[i] = 0; rv[i] = 0;
       if (i < n_pin) {
         const int32_t net = __ldg(p.pin_net + p0 + i);
-        int v;
-        bool wave = false;
+        const uint8_t pf = __ldg(p.pin_flags + p0 + i);
+        if (pf & 4) clock_mask |= 1u << i;
+        int v = pf & 3;
         if (net >= 0) {
           const int64_t a = __ldg(p.net_off + net), e = __ldg(p.net_off + net + 1);
           if (a < 0 || e < a || e > p.n_event) {
             atomicOr(p.status, kErrNetRange);
           } else if (e > a) {
-            wave = true;
-            lo[i] = a; hi[i] = e;
+            has_wave |= 1u << i;
             const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
-            g0[i] = base == 0 ? a : -1;
+            // lower_bound(T0) in [a, e)
+            int64_t l = a, r = e;
+            while (l < r) {
+              const int64_t m = l + ((r - l) >> 1);
+              if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
+            }
+            // the waveform's first event at tick 0 is the initial condition
+            if (l < e && l == a && base == 0 && ev_time(p.ev_t, l) == 0) ++l;
+            if (l > a) {
+              v = ev_value(p.ev_v, l - 1);
+            } else {
+              v = 2;
+              if (base != 0) atomicOr(p.status, kErrContext);
+              at_lo |= 1u << i;
+            }
+            // last event strictly before T0 (clamped to the first listed one)
+            const int64_t re = l > a ? l - 1 : a;
+            const int64_t pe = re > a ? re - 1 : a;
+            const int64_t tre = ev_time(p.ev_t, re) - T0;
+            lt[i] = static_cast<int32_t>(tre < kFarBefore ? kFarBefore : (tre > INT32_MAX / 2 ? INT32_MAX / 2 : tre));
+            if (nrise2(ev_value(p.ev_v, pe), ev_value(p.ev_v, re)) > 0) last_rise |= 1u << i;
+            f[i] = l;
+            rem[i] = static_cast<int32_t>(e - l);
+            if (l < e) {
+              if (RING) {
+                need |= 1u << i;
+              } else {
+                nt[i] = rel(ev_time(p.ev_t, l));
+                if (i < 16) nvals |= static_cast<uint32_t>(ev_value(p.ev_v, l)) << (2 * i);
+                else nvals_hi |= static_cast<uint64_t>(ev_value(p.ev_v, l)) << (2 * (i - 16));
+              }
+            }
           }
         }
-        if (!wave) {
-          v = __ldg(p.pin_flags + p0 + i) & 3;
-        } else {
-          has_wave |= 1u << i;
-          // lower_bound(T0) in [lo, hi)
-          int64_t l = lo[i], r = hi[i];
-          while (l < r) {
-            const int64_t m = l + ((r - l) >> 1);
-            if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
-          }
-          // an event at tick 0 that is the waveform's first is the initial condition
-          if (l < hi[i] && l == g0[i] && ev_time(p.ev_t, l) == 0) ++l;
-          f[i] = l;
-          if (l > lo[i]) {
-            v = ev_value(p.ev_v, l - 1);
-          } else {
-            v = 2;
-            if (g0[i] < 0) atomicOr(p.status, kErrContext);
-          }
-          nt[i] = l < hi[i] ? ev_time(p.ev_t, l) : kInf;
-        }
-        state |= static_cast<uint64_t>(v) << (2 * i);
+        set_v(state, state_hi, i, v);
         if (v == 1) ones |= 1u << i;
       }
     }
 
-    double acc_int = 0, acc_gint = 0, acc_sw = 0, acc_gsw = 0, acc_leak = 0;
-    uint32_t n_ev = 0, n_gl = 0, n_half = 0, n_rel = 0;
-    bool owns = owns_initial;
-    int64_t prev_time = 0;
-
+    if (RING) do_refills(-1);
     const float leak_const = ty.leak_const;
     const int32_t leak_off = ty.leak_off;
     auto leak_of = [&](uint32_t o) -> float {
-      return leak_off >= 0 ? __ldg(p.leak_pool + leak_off + o) : leak_const;
+      return leak_off >= 0 ? leak_pool[leak_off + o] : leak_const;
+    };
+    double acc_int = 0, acc_gint = 0, acc_sw = 0, acc_gsw = 0, acc_leak = 0;
+    uint32_t n_ev = 0, n_gl = 0, n_half = 0, n_rel = 0;
+    float leak_cur = leak_of(ones);
+    if (owns_initial) {
+      acc_leak += static_cast<double>(leak_cur) * static_cast<double>(p.tmax);
+      add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak_cur) * P, p.fx_leak));
+    }
+    // drift path: a segment whose seconds cycle precedes its tick cycle
+    // needs its end before its correction is known
+    bool pend = false;
+    int64_t pend_p = 0, pend_c0 = 0;
+    float pend_v = 0.0f;
+    auto apply_pending = [&](int64_t q) {
+      const double ps = static_cast<double>(pend_p) * p.ts;
+      const double qs = static_cast<double>(q) * p.ts;
+      const double b0 = static_cast<double>(pend_c0) * P;
+      const double v = static_cast<double>(pend_v);
+      if (qs < b0) {
+        add_bin(p, bins, kLeakPart, pend_c0 - 1, to_fx(-v * (qs - ps), p.fx_leak));
+      } else {
+        add_bin(p, bins, kLeakPart, pend_c0 - 1, to_fx(-v * (b0 - ps), p.fx_leak));
+        add_bin(p, bins, kLeakPart, pend_c0, to_fx(v * (b0 - ps), p.fx_leak));
+      }
+      pend = false;
     };
 
     while (true) {
-      int64_t cur = kInf;
+      uint32_t cur = kRelInf;
 #pragma unroll
       for (int i = 0; i < MAXP; ++i)
         if (i < n_pin) cur = min(cur, nt[i]);
-      if (cur >= T1) {
-        if (owns) {
-          const int64_t end = (cur == kInf) ? p.tmax : cur;
-          if (end > prev_time) {
-            const float lv = leak_of(ones);
-            acc_leak += static_cast<double>(lv) * static_cast<double>(end - prev_time);
-            W.leak_segment(prev_time, end, lv);
-          }
-        }
-        break;
-      }
-      if (cur > p.tmax) atomicOr(p.status, kErrTimeRange);
+      if (cur >= span) break;
+      const int64_t cur_abs = T0 + cur;
+      const int64_t cyc = div_floor_pos(cur_abs, p.tpc, p.inv_tpc);
+      const int32_t cs_rel = static_cast<int32_t>(cyc * p.tpc - T0);   // cycle start - T0
+      const int32_t ce_rel = cs_rel + static_cast<int32_t>(p.tpc);
+
       // advance every pin with an event at cur
-      uint64_t new_state = state;
-      uint32_t new_ones = ones;
+      const uint32_t old_state = state;
+      const uint64_t old_state_hi = state_hi;
+      const uint32_t old_ones = ones;
       uint32_t trig = 0;
 #pragma unroll
       for (int i = 0; i < MAXP; ++i) {
-        if (i < n_pin && nt[i] == cur) {
-          const int v = ev_value(p.ev_v, f[i]);
-          new_state = (new_state & ~(3ull << (2 * i))) | (static_cast<uint64_t>(v) << (2 * i));
-          new_ones = (new_ones & ~(1u << i)) | (v == 1 ? (1u << i) : 0u);
+        if (RING && i < n_pin && nt[i] == cur) {
+          const uint32_t h = rs[i] & 0xffu, held = rs[i] >> 8;
+          const int v = static_cast<int>((rv[i] >> (2 * h)) & 3u);
+          set_v(state, state_hi, i, v);
+          ones = (ones & ~(1u << i)) | (v == 1 ? (1u << i) : 0u);
+          trig |= 1u << i;
+          if (held > 1) {
+            rs[i] = (h + 1) | ((held - 1) << 8);
+            nt[i] = ring[(i * kRing + h + 1) * nt_blk + threadIdx.x];
+          } else if (rem[i] > 0) {
+            need |= 1u << i;
+            nt[i] = kRelInf;
+          } else {
+            rs[i] = 0;
+            nt[i] = kRelInf;
+          }
+          if (nt[i] <= cur) { atomicOr(p.status, kErrTimeOrder); nt[i] = kRelInf; rem[i] = 0; rs[i] = 0; }
+        } else if (!RING && i < n_pin && nt[i] == cur) {
+          const int v = get_v(nvals, nvals_hi, i);
+          set_v(state, state_hi, i, v);
+          ones = (ones & ~(1u << i)) | (v == 1 ? (1u << i) : 0u);
           trig |= 1u << i;
           ++f[i];
-          if (f[i] < hi[i]) {
+          --rem[i];
+          if (rem[i] > 0) {
             const int64_t tn = ev_time(p.ev_t, f[i]);
-            if (tn <= cur) { atomicOr(p.status, kErrTimeOrder); nt[i] = kInf; }
-            else nt[i] = tn;
+            if (tn <= cur_abs) { atomicOr(p.status, kErrTimeOrder); nt[i] = kRelInf; rem[i] = 0; }
+            else {
+              nt[i] = rel(tn);
+              if (tn > p.tmax) atomicOr(p.status, kErrTimeRange);
+              const int nv = ev_value(p.ev_v, f[i]);
+              if (i < 16) nvals = (nvals & ~(3u << (2 * i))) | (static_cast<uint32_t>(nv) << (2 * i));
+              else nvals_hi = (nvals_hi & ~(3ull << (2 * (i - 16)))) | (static_cast<uint64_t>(nv) << (2 * (i - 16)));
+            }
           } else {
-            nt[i] = kInf;
+            nt[i] = kRelInf;
           }
         }
       }
-      // leakage of the state before cur
-      if (owns) {
-        const float lv = leak_of(ones);
-        acc_leak += static_cast<double>(lv) * static_cast<double>(cur - prev_time);
-        W.leak_segment(prev_time, cur, lv);
-      }
-      const int64_t cyc = div_floor_pos(cur, p.tpc, p.inv_tpc);
-      const int64_t cyc_start = cyc * p.tpc;
-      const int64_t cyc_end = cyc_start + p.tpc;
 
+      if (RING) do_refills(static_cast<int64_t>(cur));
+
+      // leakage: level change at cur
+      if (DRIFT && pend) apply_pending(cur_abs);
+      const float leak_new = leak_of(ones);
+      const int64_t s = DRIFT ? seconds_cycle(p, cur_abs, cyc) : cyc;
+      if (leak_new != leak_cur) {
+        const double dl = static_cast<double>(leak_new) - static_cast<double>(leak_cur);
+        const double cur_s = static_cast<double>(cur_abs) * p.ts;
+        const double end_s = fmin(static_cast<double>(s + 1) * P, p.tmax_s);
+        add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin(p, bins, kLeakLevel, s + 1, to_fx(dl * P, p.fx_leak));
+        acc_leak += dl * static_cast<double>(p.tmax - cur_abs);
+      }
+      if (DRIFT && s != cyc) {
+        if (s == cyc + 1) {
+          const double w = static_cast<double>(cur_abs) * p.ts - static_cast<double>(cyc + 1) * P;
+          const double v = static_cast<double>(leak_new);
+          add_bin(p, bins, kLeakPart, cyc, to_fx(-v * w, p.fx_leak));
+          add_bin(p, bins, kLeakPart, cyc + 1, to_fx(v * w, p.fx_leak));
+        } else {
+          pend = true;
+          pend_p = cur_abs;
+          pend_c0 = cyc;
+          pend_v = leak_new;
+        }
+      }
+      leak_cur = leak_new;
+
+      // energies of the triggered pins, in pin order, from the pre-step state
       uint32_t tb = trig;
       while (tb) {
         const int i = __ffs(tb) - 1;
         tb &= tb - 1;
-        const int pv = static_cast<int>((state >> (2 * i)) & 3);
-        const int nv = static_cast<int>((new_state >> (2 * i)) & 3);
+        const int pv = get_v(old_state, old_state_hi, i);
+        const int nv = get_v(state, state_hi, i);
         const int tog2 = ntoggle2(pv, nv);
         const int nr2 = nrise2(pv, nv);
         const bool rise = nr2 > 0;
-        const int pin = p0 + i;
-        const uint8_t pf = __ldg(p.pin_flags + pin);
 
-        // ---- glitch classification and ratio ----
+        // glitch: the event is isolated in its period unless its previous
+        // event (strictly before) or its next event shares the period
         float g = -1.0f;
-        const int64_t e = sel(f, i) - 1;
-        const int64_t lo_i = sel(lo, i), hi_i = sel(hi, i), g0_i = sel(g0, i);
-        if (!(pf & 4) && e != g0_i) {
-          const Group gr = period_group(p.ev_t, e, lo_i, hi_i, g0_i, cyc_start, cyc_end);
-          const int64_t k = gr.last - gr.first + 1;
-          const int64_t lim = k >= 2 ? (k & ~int64_t(1)) : 0;
-          if (e - gr.first < lim) {
-            int64_t w = -1;
-            // previous event flagged?
-            if (e - 1 >= lo_i && e != g0_i) {
-              bool pflag;
-              if (e - 1 >= gr.first) {
-                pflag = true;
-              } else if (e - 1 == g0_i) {
-                pflag = false;
-              } else {
-                const int64_t tp = ev_time(p.ev_t, e - 1);
-                const int64_t pc = div_floor_pos(tp, p.tpc, p.inv_tpc);
-                const Group gp = period_group(p.ev_t, e - 1, lo_i, hi_i, g0_i, pc * p.tpc,
-                                              pc * p.tpc + p.tpc);
-                const int64_t kp = gp.last - gp.first + 1;   // e-1 is the last of its period
-                pflag = kp >= 2 && (kp & 1) == 0;
-              }
-              if (pflag) w = cur - ev_time(p.ev_t, e - 1);
-            }
-            if (e + 1 < hi_i) {
-              bool nflag;
-              const int64_t tn = ev_time(p.ev_t, e + 1);
-              if (e + 1 <= gr.last) {
-                nflag = (e + 1 - gr.first) < lim;
-              } else if (e + 2 < hi_i) {
-                const int64_t nc = div_floor_pos(tn, p.tpc, p.inv_tpc);
-                nflag = ev_time(p.ev_t, e + 2) < nc * p.tpc + p.tpc;
-              } else {
-                nflag = false;
-              }
-              if (nflag) w = max(w, tn - cur);
-            }
-            if (w >= 0) {
-              const float den = __ldg(p.pin_gden + pin);
-              if (den == 0.0f) {
-                g = 1.0f;
-              } else {
-                const float pw = __double2float_rn(__dmul_rn(static_cast<double>(w), p.ts));
-                const float r = __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(pw), 2.0),
-                                                            static_cast<double>(den)));
-                g = fminf(1.0f, __fmul_rn(r, r));
-              }
-            }
+        if (!((clock_mask >> i) & 1)) {
+          const bool prev_same = !((at_lo >> i) & 1) && sel<MAXP>(lt, i) >= cs_rel;
+          const uint32_t nti = sel<MAXP>(nt, i);
+          const bool next_same = nti == kRelBeyond || (nti != kRelInf && static_cast<int32_t>(nti) < ce_rel);
+          if (prev_same || next_same) {
+            const int32_t net = __ldg(p.pin_net + p0 + i);
+            const int64_t lo = __ldg(p.net_off + net), hi = __ldg(p.net_off + net + 1);
+            const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
+            const int64_t ev_idx = RING ? sel<MAXP>(f, i) - static_cast<int64_t>(sel<MAXP>(rs, i) >> 8) - 1
+                                        : sel<MAXP>(f, i) - 1;
+            g = glitch_ratio(p, ev_idx, lo, hi, base == 0 ? lo : -1, cur_abs,
+                             cyc * p.tpc, __ldg(p.pin_gden + p0 + i));
           }
         }
 
-        // ---- internal energy ----
         float energy = 0.0f;
-        const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + i);
-        const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + i + 1);
         if (i < n_in) {
-          for (int32_t s = s_begin; s < s_end; ++s) {
-            const DevSlot sl = p.slots[s];
-            if (when_holds(p.cubes, sl.cube_off, sl.n_cube, ones)) {
-              energy = __ldg(blk + sl.e_off + (rise ? 0 : 1));
-              break;
+          if (FAST) {
+            const int16_t eo = fast_tab[fo + i * n_state + old_ones];
+            if (eo >= 0) energy = blk[eo + (rise ? 0 : 1)];
+          } else {
+            const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + i);
+            const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + i + 1);
+            for (int32_t k = s_begin; k < s_end; ++k) {
+              const DevSlot sl = p.slots[k];
+              if (when_holds(p.cubes, sl.cube_off, sl.n_cube, old_ones)) {
+                energy = blk[sl.e_off + (rise ? 0 : 1)];
+                break;
+              }
             }
           }
         } else {
           const int o = i - n_in;
           float best = p.min_diff0;
-          int rel = -1;
+          int relq = -1;
           bool rel_rise = false;
-          const double cur_s = __dmul_rn(static_cast<double>(cur), p.ts);
-          for (int q = 0; q < n_in; ++q) {
+          const double cur_s = __dmul_rn(static_cast<double>(cur_abs), p.ts);
+          const float* dlp = blk + ty.delay_off + o * n_in * 4 + (rise ? 0 : 1);
+#pragma unroll
+          for (int q = 0; q < (MAXP < 2 ? 1 : MAXP - 1); ++q) {
+            if (q >= n_in) break;
             if (!((has_wave >> q) & 1)) continue;
-            // lower_bound(cur) on pin q: its frontier, minus one if q fired at cur
-            const int64_t lb = sel(f, q) - ((trig >> q) & 1);
-            const int64_t loq = sel(lo, q);
-            const int64_t re = max(loq, lb - 1);
-            const int64_t pe = max(loq, re - 1);
-            const bool fr = nrise2(ev_value(p.ev_v, pe), ev_value(p.ev_v, re)) > 0;
-            const float dl = __ldg(blk + ty.delay_off + (o * n_in + q) * 4 + (fr ? 0 : 2) + (rise ? 0 : 1));
+            const bool fr = (last_rise >> q) & 1;
+            const float dl = dlp[q * 4 + (fr ? 0 : 2)];
             if (isnan(dl)) continue;
-            const int64_t tr = ev_time(p.ev_t, re);
-            const double a = __dsub_rn(cur_s, static_cast<double>(dl));
-            const float diff = __double2float_rn(fabs(__dsub_rn(a, __dmul_rn(static_cast<double>(tr), p.ts))));
-            if (diff < best && tr >= cyc_start && tr < cyc_end) {
+            const int32_t tr = lt[q];
+            const double trs = __dmul_rn(static_cast<double>(T0 + tr), p.ts);
+            const float diff = __double2float_rn(fabs(__dsub_rn(__dsub_rn(cur_s, static_cast<double>(dl)), trs)));
+            if (diff < best && tr >= cs_rel && tr < ce_rel) {
               best = diff;
-              rel = q;
+              relq = q;
               rel_rise = fr;
             }
           }
-          if (rel < 0) {
-            energy = __ldg(blk + ty.def_off + 2 * o + (rise ? 0 : 1));
+          if (relq < 0) {
+            energy = blk[ty.def_off + 2 * o + (rise ? 0 : 1)];
+          } else if (FAST) {
+            const int16_t eo = fast_tab[fo + n_in * n_state + (o * n_in + relq) * n_state + old_ones];
+            if (eo >= 0) energy = blk[eo + (rel_rise ? 0 : 2) + (rise ? 0 : 1)];
           } else {
-            for (int32_t s = s_begin; s < s_end; ++s) {
-              const DevSlot sl = p.slots[s];
-              if (sl.related != rel) continue;
-              if (when_holds(p.cubes, sl.cube_off, sl.n_cube, ones)) {
-                energy = __ldg(blk + sl.e_off + (rel_rise ? 0 : 2) + (rise ? 0 : 1));
+            const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + i);
+            const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + i + 1);
+            for (int32_t k = s_begin; k < s_end; ++k) {
+              const DevSlot sl = p.slots[k];
+              if (sl.related != relq) continue;
+              if (when_holds(p.cubes, sl.cube_off, sl.n_cube, old_ones)) {
+                energy = blk[sl.e_off + (rel_rise ? 0 : 2) + (rise ? 0 : 1)];
                 break;
               }
             }
           }
-          if (COUNTS) n_rel += static_cast<uint32_t>(rel + 1);
+          if (COUNTS) n_rel += static_cast<uint32_t>(relq + 1);
           // switching: n_rise * C * V^2
           if (nr2 > 0) {
-            const float esw = __fmul_rn(nr2 == 2 ? 1.0f : 0.5f, __ldg(p.pin_swe + pin));
+            const float esw = __fmul_rn(nr2 == 2 ? 1.0f : 0.5f, __ldg(p.pin_swe + p0 + i));
             if (g > 0.0f) {
               const float x = __fmul_rn(g, esw);
               acc_gsw += x;
-              W.add_cyc(5, cyc, x, p.fx_dyn);
+              add_bin(p, bins, kGSw, cyc, to_fx(x, p.fx_dyn));
             } else {
               acc_sw += esw;
-              W.add_cyc(4, cyc, esw, p.fx_dyn);
+              add_bin(p, bins, kSw, cyc, to_fx(esw, p.fx_dyn));
             }
           }
         }
@@ -448,22 +626,39 @@ __global__ void __launch_bounds__(256) power_walk_kernel(const KParams p) {
         if (g > 0.0f) {
           const float x = __fmul_rn(g, energy);
           acc_gint += x;
-          W.add_cyc(3, cyc, x, p.fx_dyn);
-          if (COUNTS) { ++n_gl; W.add_cnt(1, cyc); }
+          add_bin(p, bins, kGInt, cyc, to_fx(x, p.fx_dyn));
+          if (COUNTS) { ++n_gl; add_cnt(p, bins, 1, cyc); }
         } else {
           acc_int += energy;
-          W.add_cyc(2, cyc, energy, p.fx_dyn);
+          add_bin(p, bins, kInt, cyc, to_fx(energy, p.fx_dyn));
         }
         if (COUNTS) {
           ++n_ev;
           n_half += static_cast<uint32_t>(tog2);
-          W.add_cnt(0, cyc);
+          add_cnt(p, bins, 0, cyc);
         }
       }
-      state = new_state;
-      ones = new_ones;
-      prev_time = cur;
-      owns = true;
+      // the triggered pins' last event is now cur
+#pragma unroll
+      for (int i = 0; i < MAXP; ++i) {
+        if ((trig >> i) & 1) {
+          const bool r = !((at_lo >> i) & 1) &&
+                         nrise2(get_v(old_state, old_state_hi, i), get_v(state, state_hi, i)) > 0;
+          last_rise = (last_rise & ~(1u << i)) | (r ? (1u << i) : 0u);
+          lt[i] = static_cast<int32_t>(cur);
+        }
+      }
+      at_lo &= ~trig;
+    }
+
+    if (DRIFT && pend) {
+      // end of the pending segment: the cell's next event, or time_max
+      int64_t q = p.tmax;
+#pragma unroll
+      for (int i = 0; i < MAXP; ++i)
+        if (i < n_pin && nt[i] != kRelInf)
+          q = min(q, ev_time(p.ev_t, RING ? f[i] - static_cast<int64_t>(rs[i] >> 8) : f[i]));
+      apply_pending(q);
     }
 
     // flush the cell's sums for this tile
@@ -499,6 +694,51 @@ __global__ void __launch_bounds__(256) power_walk_kernel(const KParams p) {
     }
   }
 }
+
+// ---- walk order by work ----
+
+__global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
+                                 int32_t b1, int32_t b2, unsigned long long* __restrict__ keys) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int32_t cell = base_order[k];
+  const int32_t a = p.cell_pin_off[cell], e = p.cell_pin_off[cell + 1];
+  long long w = 0;
+  for (int32_t q = a; q < e; ++q) {
+    const int32_t net = p.pin_net[q];
+    if (net >= 0) w += p.net_off[net + 1] - p.net_off[net];
+  }
+  const unsigned long long bucket = k >= b2 ? 2ull : (k >= b1 ? 1ull : 0ull);
+  const unsigned long long cap = (1ull << 40) - 1;
+  const unsigned long long wc = w < 0 ? 0ull : (static_cast<unsigned long long>(w) > cap ? cap : static_cast<unsigned long long>(w));
+  keys[k] = (bucket << 40) | (cap - wc);
+}
+
+}  // namespace
+
+size_t work_sort_temp_bytes(int32_t n_cell) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const unsigned long long*>(nullptr),
+                                  static_cast<unsigned long long*>(nullptr),
+                                  static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
+                                  n_cell, 0, 42);
+  return bytes;
+}
+
+cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int32_t n_cell,
+                               const int32_t* bucket_begin, unsigned long long* keys_in,
+                               unsigned long long* keys_out, int32_t* order_out, void* temp,
+                               size_t temp_bytes, cudaStream_t stream) {
+  if (n_cell <= 0) return cudaSuccess;
+  work_keys_kernel<<<(n_cell + 255) / 256, 256, 0, stream>>>(p, base_order, n_cell, bucket_begin[1],
+                                                             bucket_begin[2], keys_in);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, base_order, order_out,
+                                         n_cell, 0, 42, stream);
+}
+
+namespace {
 
 // ---- finalize ----
 
@@ -537,14 +777,14 @@ __global__ void finalize_cells(const KParams p, const uint8_t* __restrict__ grou
   if (threadIdx.x < (GTP_N_GROUP + 1) * 5) atomicAdd(tg + threadIdx.x, (&red[0][0])[threadIdx.x]);
 }
 
-// One block: prefix-sums the leakage run-differences and converts the
-// fixed-point per-cycle energies to watts.
+// One block: prefix-sums the leakage level differences and converts the
+// fixed-point per-cycle energies to watts. The level of cycle c covers the
+// part of the cycle before time_max.
 __global__ void finalize_cycles(const KParams p, float* __restrict__ cycle5,
                                 unsigned long long* __restrict__ leak_tmp) {
   const int64_t np = p.n_period;
   const int64_t stride = np + 1;
   const unsigned long long* acc = p.cyc_acc;
-  // block-wide inclusive scan of the run-difference array, chunked
   __shared__ unsigned long long carry_s;
   __shared__ unsigned long long warp_sums[32];
   if (threadIdx.x == 0) carry_s = 0;
@@ -552,7 +792,7 @@ __global__ void finalize_cycles(const KParams p, float* __restrict__ cycle5,
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int64_t base = 0; base < np; base += blockDim.x) {
     const int64_t c = base + threadIdx.x;
-    unsigned long long x = c < np ? acc[1 * stride + c] : 0ull;
+    unsigned long long x = c < np ? acc[kLeakLevel * stride + c] : 0ull;
     for (int o = 1; o < 32; o <<= 1) {
       unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += y;
@@ -575,15 +815,20 @@ __global__ void finalize_cycles(const KParams p, float* __restrict__ cycle5,
     if (threadIdx.x == blockDim.x - 1) carry_s = pre;
     __syncthreads();
   }
-  const double inv_l = 1.0 / (p.fx_leak * p.period_d);
-  const double inv_d = 1.0 / (p.fx_dyn * p.period_d);
+  const double P = p.period_d;
+  const double inv_l = 1.0 / (p.fx_leak * P);
+  const double inv_d = 1.0 / (p.fx_dyn * P);
   for (int64_t c = threadIdx.x; c < np; c += blockDim.x) {
-    const long long lk = static_cast<long long>(acc[0 * stride + c] + leak_tmp[c]);
-    const long long ir = static_cast<long long>(acc[2 * stride + c]);
-    const long long ig = static_cast<long long>(acc[3 * stride + c]);
-    const long long sr = static_cast<long long>(acc[4 * stride + c]);
-    const long long sg = static_cast<long long>(acc[5 * stride + c]);
-    cycle5[0 * np + c] = static_cast<float>(static_cast<double>(lk) * inv_l);
+    const double c0 = static_cast<double>(c) * P;
+    double frac = (fmin(static_cast<double>(c + 1) * P, p.tmax_s) - c0) / P;
+    frac = frac < 0.0 ? 0.0 : (frac > 1.0 ? 1.0 : frac);
+    const double level = static_cast<double>(static_cast<long long>(leak_tmp[c]));
+    const double part = static_cast<double>(static_cast<long long>(acc[kLeakPart * stride + c]));
+    const long long ir = static_cast<long long>(acc[kInt * stride + c]);
+    const long long ig = static_cast<long long>(acc[kGInt * stride + c]);
+    const long long sr = static_cast<long long>(acc[kSw * stride + c]);
+    const long long sg = static_cast<long long>(acc[kGSw * stride + c]);
+    cycle5[0 * np + c] = static_cast<float>((level * frac + part) * inv_l);
     cycle5[1 * np + c] = static_cast<float>(static_cast<double>(ir + ig) * inv_d);
     cycle5[2 * np + c] = static_cast<float>(static_cast<double>(ig) * inv_d);
     cycle5[3 * np + c] = static_cast<float>(static_cast<double>(sr + sg) * inv_d);
@@ -591,12 +836,15 @@ __global__ void finalize_cycles(const KParams p, float* __restrict__ cycle5,
   }
 }
 
-template <int MAXP, bool COUNTS>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
 cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   const int32_t n = p.order_end - p.order_begin;
   if (n <= 0) return cudaSuccess;
-  const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS);
-  auto kern = power_walk_kernel<MAXP, COUNTS>;
+  size_t tabs = (FAST && p.tabs_in_smem) ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16 : 0;
+  if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
+  const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads,
+                                            (FAST && WALK_USE_RING) ? MAXP : 0, tabs);
+  auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -607,15 +855,31 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
 
 }  // namespace
 
-size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts) {
-  return static_cast<size_t>(cycles_per_tile) * (kNumCycAcc * 8 + (counts ? 8 : 0));
+size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
+                             size_t tab_bytes) {
+  return static_cast<size_t>(cycles_per_tile) * (kNumCycAcc * 8 + (counts ? 8 : 0)) +
+         static_cast<size_t>(ring_pins) * kRing * threads * 4 + tab_bytes;
 }
 
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
                               cudaStream_t stream) {
-  if (max_pins <= 4) return counts ? launch_t<4, true>(p, threads, stream) : launch_t<4, false>(p, threads, stream);
-  if (max_pins <= 8) return counts ? launch_t<8, true>(p, threads, stream) : launch_t<8, false>(p, threads, stream);
-  return counts ? launch_t<kMaxPins, true>(p, threads, stream) : launch_t<kMaxPins, false>(p, threads, stream);
+  const bool d = p.drift != 0;
+  if (max_pins <= kFastPins) {
+    if (d) return counts ? launch_t<kFastPins, true, true, true>(p, threads, stream)
+                         : launch_t<kFastPins, false, true, true>(p, threads, stream);
+    return counts ? launch_t<kFastPins, true, true, false>(p, threads, stream)
+                  : launch_t<kFastPins, false, true, false>(p, threads, stream);
+  }
+  if (max_pins <= 8) {
+    if (d) return counts ? launch_t<8, true, false, true>(p, threads, stream)
+                         : launch_t<8, false, false, true>(p, threads, stream);
+    return counts ? launch_t<8, true, false, false>(p, threads, stream)
+                  : launch_t<8, false, false, false>(p, threads, stream);
+  }
+  if (d) return counts ? launch_t<kMaxPins, true, false, true>(p, threads, stream)
+                       : launch_t<kMaxPins, false, false, true>(p, threads, stream);
+  return counts ? launch_t<kMaxPins, true, false, false>(p, threads, stream)
+                : launch_t<kMaxPins, false, false, false>(p, threads, stream);
 }
 
 cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,

@@ -373,6 +373,229 @@ void synth_pack_values(const uint8_t* values, int64_t n, uint32_t* packed, int32
   for (auto& x : th) x.join();
 }
 
+// ---------------------------------------------------------------------------
+// Streaming: cycle windows with the context the power walk reads.
+//
+// Window k covers cycles [c_lo, c_hi). Besides its own events, each net
+// lists (a) the events of the last clock period before c_lo that has any
+// and the event before that period, and (b) the first events at or after
+// c_hi that the glitch look-ahead can read: the next window's events are
+// generated one call ahead and supply them; a net with none there is
+// scanned further only when its last listed period ends in a glitch event
+// (an even count of at least two), the only case in which the look-ahead
+// reads past the window.
+void synth_trace_initial(void* h, uint8_t* init_value);
+
+namespace {
+
+struct Stream {
+  Trace* tr = nullptr;
+  int64_t wcyc = 0;
+  int32_t n_threads = 1;
+  int64_t c_next = 0;                 // first cycle of the next window to emit
+  std::vector<uint8_t> value_gen;     // net value after the last generated cycle
+  std::vector<int64_t> gcount;        // events emitted in bodies so far, per net
+  std::vector<int64_t> ring_t;        // [net][4] head context
+  std::vector<uint8_t> ring_v;
+  std::vector<uint8_t> ring_n;
+  std::vector<uint8_t> ring_g0;       // ring's first event is the waveform's first
+  // generated bodies: current (to emit) and next (look-ahead)
+  std::vector<int64_t> b_off[2], b_t[2];
+  std::vector<uint8_t> b_v[2];
+  int64_t b_lo[2] = {0, 0}, b_hi[2] = {0, 0};
+  int cur = 0;
+  bool have[2] = {false, false};
+};
+
+void gen_body(Stream& s, int slot, int64_t c_lo, int64_t c_hi) {
+  Trace& tr = *s.tr;
+  const int32_t nn = tr.tp.n_net;
+  std::vector<int64_t>& off = s.b_off[slot];
+  off.assign(nn + 1, 0);
+  std::vector<int64_t> cnt(nn);
+  synth_trace_count(&tr, c_lo, c_hi, cnt.data(), s.n_threads);
+  for (int32_t n = 0; n < nn; ++n) off[n + 1] = off[n] + cnt[n];
+  s.b_t[slot].resize(off[nn]);
+  s.b_v[slot].resize(off[nn]);
+  synth_trace_fill(&tr, c_lo, c_hi, off.data(), s.value_gen.data(), s.b_t[slot].data(),
+                   s.b_v[slot].data(), s.n_threads);
+  s.b_lo[slot] = c_lo;
+  s.b_hi[slot] = c_hi;
+  s.have[slot] = true;
+}
+
+}  // namespace
+
+void* synth_stream_create(void* trace, int64_t window_cycles, int32_t n_threads) {
+  Trace* tr = static_cast<Trace*>(trace);
+  Stream* s = new Stream();
+  s->tr = tr;
+  s->wcyc = std::max<int64_t>(1, window_cycles);
+  s->n_threads = std::max(1, n_threads);
+  const int32_t nn = tr->tp.n_net;
+  s->value_gen.resize(nn);
+  synth_trace_initial(tr, s->value_gen.data());
+  s->gcount.assign(nn, 0);
+  s->ring_t.assign(4 * static_cast<size_t>(nn), 0);
+  s->ring_v.assign(4 * static_cast<size_t>(nn), 0);
+  s->ring_n.assign(nn, 0);
+  s->ring_g0.assign(nn, 0);
+  return s;
+}
+
+void synth_stream_free(void* h) { delete static_cast<Stream*>(h); }
+
+// Emits the next window into caller buffers (times, one value byte per
+// event, net_off [n_net+1], net_base [n_net]) of capacity `cap` events.
+// Returns the number of events written, 0 when the trace is exhausted, or
+// -(events needed) when cap is too small (nothing is consumed then).
+int64_t synth_stream_next(void* h, int64_t* t_lo, int64_t* t_hi, int64_t* net_off, int64_t* times,
+                          uint8_t* values, int64_t* net_base, int64_t cap) {
+  Stream& s = *static_cast<Stream*>(h);
+  Trace& tr = *s.tr;
+  const int64_t nc = tr.tp.n_cycle;
+  const int32_t nn = tr.tp.n_net;
+  if (s.c_next >= nc) return 0;
+  const int a = s.cur, b = 1 - s.cur;
+  const int64_t c_lo = s.c_next;
+  const int64_t c_hi = std::min(nc, c_lo + s.wcyc);
+  if (!s.have[a]) gen_body(s, a, c_lo, c_hi);
+  if (c_hi < nc && !s.have[b]) gen_body(s, b, c_hi, std::min(nc, c_hi + s.wcyc));
+  const int64_t tpc = tr.tp.tpc;
+  // per-net layout
+  std::vector<int64_t> tail_n(nn, 0);
+  std::vector<int64_t> tail_t(2 * static_cast<size_t>(nn));
+  std::vector<uint8_t> tail_v(2 * static_cast<size_t>(nn));
+  auto period_of = [&](int64_t t) { return t / tpc; };
+  auto job = [&](int tid) {
+    int64_t tbuf[3];
+    for (int32_t n = tid; n < nn; n += s.n_threads) {
+      // events of the last listed period: body's last cycle, else the ring
+      const int64_t bo = s.b_off[a][n], be = s.b_off[a][n + 1];
+      int k_last = 0;
+      bool g0_in = false;
+      if (be > bo) {
+        const int64_t pl = period_of(s.b_t[a][be - 1]);
+        int64_t j = be - 1;
+        while (j >= bo && period_of(s.b_t[a][j]) == pl) { ++k_last; --j; }
+        g0_in = (c_lo == 0 && pl == 0);  // the tick-0 initial value is not counted
+      } else if (c_lo > 0 && s.ring_n[n] > 0) {
+        const int rn = s.ring_n[n];
+        const int64_t pl = period_of(s.ring_t[4 * n + rn - 1]);
+        for (int j = rn - 1; j >= 0 && period_of(s.ring_t[4 * n + j]) == pl; --j) ++k_last;
+        g0_in = s.ring_g0[n] && period_of(s.ring_t[4 * n]) == pl;
+      }
+      const int k_eff = k_last - (g0_in ? 1 : 0);
+      const bool need_far = k_eff >= 2 && (k_eff % 2) == 0;
+      int64_t tn = 0;
+      if (c_hi < nc) {
+        const int64_t no = s.b_off[b][n], ne = s.b_off[b][n + 1];
+        for (int64_t j = no; j < ne && tn < 2; ++j) {
+          tail_t[2 * n + tn] = s.b_t[b][j];
+          tail_v[2 * n + tn] = s.b_v[b][j];
+          ++tn;
+        }
+        if (tn == 0 && need_far) {
+          // scan past the look-ahead window for the next period with events
+          uint8_t v = s.value_gen[n];
+          for (int64_t c = s.b_hi[b]; c < nc && tn == 0; ++c) {
+            const int m = cycle_events(tr, n, c, tbuf);
+            for (int j = 0; j < m && tn < 2; ++j) {
+              v ^= 1;
+              tail_t[2 * n + tn] = tbuf[j];
+              tail_v[2 * n + tn] = v;
+              ++tn;
+            }
+          }
+        }
+      }
+      tail_n[n] = tn;
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (int i = 0; i < s.n_threads; ++i) th.emplace_back(job, i);
+    for (auto& x : th) x.join();
+  }
+  net_off[0] = 0;
+  for (int32_t n = 0; n < nn; ++n) {
+    const int64_t head = c_lo > 0 ? s.ring_n[n] : 0;
+    net_off[n + 1] = net_off[n] + head + (s.b_off[a][n + 1] - s.b_off[a][n]) + tail_n[n];
+  }
+  const int64_t total = net_off[nn];
+  if (total > cap) return -total;
+  auto fill = [&](int tid) {
+    for (int32_t n = tid; n < nn; n += s.n_threads) {
+      int64_t k = net_off[n];
+      const int64_t head = c_lo > 0 ? s.ring_n[n] : 0;
+      for (int64_t j = 0; j < head; ++j) {
+        times[k] = s.ring_t[4 * n + j];
+        values[k] = s.ring_v[4 * n + j];
+        ++k;
+      }
+      for (int64_t j = s.b_off[a][n]; j < s.b_off[a][n + 1]; ++j) {
+        times[k] = s.b_t[a][j];
+        values[k] = s.b_v[a][j];
+        ++k;
+      }
+      for (int64_t j = 0; j < tail_n[n]; ++j) {
+        times[k] = tail_t[2 * n + j];
+        values[k] = tail_v[2 * n + j];
+        ++k;
+      }
+      net_base[n] = s.gcount[n] - head;
+      // new ring: last non-empty period of the body plus the event before it
+      const int64_t bo = s.b_off[a][n], be = s.b_off[a][n + 1];
+      if (be > bo) {
+        const int64_t pl = period_of(s.b_t[a][be - 1]);
+        int64_t j = be - 1;
+        while (j - 1 >= bo && period_of(s.b_t[a][j - 1]) == pl) --j;
+        // j = first event of the last period in the body
+        int64_t src_t[4];
+        uint8_t src_v[4];
+        int m = 0;
+        bool g0 = false;
+        if (j - 1 >= bo) {
+          src_t[m] = s.b_t[a][j - 1];
+          src_v[m] = s.b_v[a][j - 1];
+          ++m;
+          g0 = (c_lo == 0 && j - 1 == bo);
+        } else if (c_lo > 0 && s.ring_n[n] > 0) {
+          src_t[m] = s.ring_t[4 * n + s.ring_n[n] - 1];
+          src_v[m] = s.ring_v[4 * n + s.ring_n[n] - 1];
+          ++m;
+          g0 = s.ring_g0[n] && s.ring_n[n] == 1;
+        } else {
+          g0 = (c_lo == 0 && j == bo);
+        }
+        for (int64_t q = j; q < be && m < 4; ++q) {
+          src_t[m] = s.b_t[a][q];
+          src_v[m] = s.b_v[a][q];
+          ++m;
+        }
+        for (int q = 0; q < m; ++q) {
+          s.ring_t[4 * n + q] = src_t[q];
+          s.ring_v[4 * n + q] = src_v[q];
+        }
+        s.ring_n[n] = static_cast<uint8_t>(m);
+        s.ring_g0[n] = g0 ? 1 : 0;
+        s.gcount[n] += be - bo;
+      }
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (int i = 0; i < s.n_threads; ++i) th.emplace_back(fill, i);
+    for (auto& x : th) x.join();
+  }
+  *t_lo = c_lo * tpc;
+  *t_hi = c_hi < nc ? c_hi * tpc : INT64_MAX;
+  s.have[a] = false;
+  s.cur = b;
+  s.c_next = c_hi;
+  return total;
+}
+
 // Initial net values (tick 0): a seeded coin per net; the clock starts at 0.
 void synth_trace_initial(void* h, uint8_t* init_value) {
   Trace* tr = static_cast<Trace*>(h);

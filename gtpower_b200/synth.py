@@ -66,6 +66,12 @@ def synth_lib() -> C.CDLL:
                                        C.c_void_p, C.c_void_p, C.c_int32]
         L.synth_trace_initial.argtypes = [C.c_void_p, C.c_void_p]
         L.synth_pack_values.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32]
+        L.synth_stream_create.restype = C.c_void_p
+        L.synth_stream_create.argtypes = [C.c_void_p, C.c_int64, C.c_int32]
+        L.synth_stream_free.argtypes = [C.c_void_p]
+        L.synth_stream_next.restype = C.c_int64
+        L.synth_stream_next.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
         _slib = L
     return _slib
 
@@ -330,3 +336,47 @@ class Trace:
         packed = np.empty((times.shape[0] + 15) // 16, dtype=np.uint32)
         synth_lib().synth_pack_values(_p(vals), times.shape[0], _p(packed), threads or os.cpu_count() or 1)
         return Events(net_off, times, packed)
+
+
+class Stream:
+    """Cycle windows of a `Trace` with the head/tail context each window
+    needs, generated one window ahead (synth_stream_next in synth.cpp)."""
+
+    def __init__(self, trace: Trace, window_cycles: int, threads: int = 0):
+        self.trace = trace
+        self.threads = threads or os.cpu_count() or 1
+        self.h = synth_lib().synth_stream_create(trace.h, window_cycles, self.threads)
+        self.n_net = trace.n_net
+
+    def __del__(self):
+        try:
+            synth_lib().synth_stream_free(self.h)
+        except Exception:
+            pass
+
+    def next_into(self, times: np.ndarray, values: np.ndarray, net_off: np.ndarray,
+                  net_base: np.ndarray):
+        """Fills caller buffers; returns (n_event, t_lo, t_hi), None at the
+        end. Raises if the buffers are too small."""
+        lo = C.c_int64()
+        hi = C.c_int64()
+        n = synth_lib().synth_stream_next(self.h, C.byref(lo), C.byref(hi), _p(net_off), _p(times),
+                                          _p(values), _p(net_base), times.shape[0])
+        if n == 0:
+            return None
+        if n < 0:
+            raise ValueError(f"stream buffers too small: {-n} events needed")
+        return int(n), lo.value, hi.value
+
+    def next(self, cap: int) -> Events | None:
+        times = np.empty(cap, np.int64)
+        values = np.empty(cap, np.uint8)
+        net_off = np.empty(self.n_net + 1, np.int64)
+        net_base = np.empty(self.n_net, np.int64)
+        r = self.next_into(times, values, net_off, net_base)
+        if r is None:
+            return None
+        n, t_lo, t_hi = r
+        packed = np.empty((n + 15) // 16, np.uint32)
+        synth_lib().synth_pack_values(_p(values), n, _p(packed), self.threads)
+        return Events(net_off, times[:n].copy(), packed, net_base=net_base, t_lo=t_lo, t_hi=t_hi)

@@ -202,7 +202,11 @@ typedef struct gtp_config {
   int32_t max_n_pin_for_leakage_power; /* 16 (GlobalConfig.hh:41) */
   int32_t collect_counts;            /* 1 = fill gtp_counts (exact parity) */
   int64_t max_event_num;             /* device event capacity (GlobalConfig.hh:31) */
-  int64_t reserved[4];
+  int32_t sort_by_work;              /* 1 = per window, walk cells in order of their
+                                        event count so a warp's cells carry similar
+                                        work (default 1) */
+  int32_t reserved32;
+  int64_t reserved[3];
 } gtp_config;
 
 /* Integer counters that must match the oracle bit-exactly. */

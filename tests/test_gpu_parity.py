@@ -65,3 +65,22 @@ def test_empty_trace():
     ev = toy.events(3, {})
     res = run_engine(d, [ev])
     compare(res, oracle(d, ev))
+
+
+@pytest.mark.parametrize("window", [9, 25])
+def test_streamed_skew_trace(window):
+    """Skewed (Zipf x burst) trace pushed window by window from the streaming
+    generator equals the oracle on the whole trace."""
+    from gtpower_b200 import synth
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=2000, n_cycle=100, seed=8))
+    spec = synth.TraceSpec(mode=1, glitch_p=0.1)
+    full = synth.Trace(d, info, spec, seed=12).full()
+    st = synth.Stream(synth.Trace(d, info, spec, seed=12), window)
+    wins = []
+    while True:
+        w = st.next(400_000)
+        if w is None:
+            break
+        wins.append(w)
+    res = run_engine(d, wins, cycles_per_tile=6)
+    compare(res, oracle(d, full))
