@@ -94,13 +94,27 @@ class gtp_counts(C.Structure):
                 ("dropped", C.c_int64)]
 
 
-# Every symbol the header declares, in order.
-EXPORTED = [
+class gtp_proxy_config(C.Structure):
+    _fields_ = [("cuda_device_id", C.c_int32), ("n_in", C.c_int32), ("n_hidden", C.c_int32),
+                ("n_out", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float), ("seed", C.c_uint64), ("use_graph", C.c_int32),
+                ("reserved32", C.c_int32), ("reserved", C.c_int64 * 4)]
+
+
+# Every symbol the headers declare (include/gtpb200.h, include/gtpb200_proxy.h).
+EXPORTED = sorted([
     "gtp_config_default", "gtp_create", "gtp_destroy", "gtp_last_error", "gtp_n_period",
     "gtp_ticks_per_cycle", "gtp_reset", "gtp_push_events", "gtp_push_events_device",
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
     "gtp_evaluate_noalloc", "gtp_pack_values",
-]
+    "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
+    "gtp_proxy_get_stream", "gtp_proxy_set_stream", "gtp_proxy_n_param",
+    "gtp_proxy_set_training_data", "gtp_proxy_get_norm", "gtp_proxy_train",
+    "gtp_proxy_compute_grads", "gtp_proxy_adam_step", "gtp_proxy_get_params",
+    "gtp_proxy_set_params", "gtp_proxy_get_grads", "gtp_proxy_predict", "gtp_toggle_bits",
+    "gtp_net_toggle_stats", "gtp_bf16_gemm",
+])
 
 _lib = None
 
@@ -150,6 +164,7 @@ def lib() -> C.CDLL:
     L.gtp_evaluate_noalloc.restype = C.c_int32
     L.gtp_pack_values.argtypes = [_P, C.c_int64, _P]
     L.gtp_pack_values.restype = None
+    _bind_proxy(L)
     _lib = L
     return L
 
@@ -164,3 +179,32 @@ def check(status: int, ctx=None) -> None:
     if status != GTP_OK:
         msg = lib().gtp_last_error(ctx)
         raise GtpError(status, msg.decode() if msg else "")
+
+
+def _bind_proxy(L: C.CDLL) -> None:
+    i32, i64, f = C.c_int32, C.c_int64, C.c_float
+    sigs = {
+        "gtp_proxy_config_default": ([C.POINTER(gtp_proxy_config)], None),
+        "gtp_proxy_create": ([C.POINTER(gtp_proxy_config), C.POINTER(C.c_void_p)], i32),
+        "gtp_proxy_destroy": ([_P], None),
+        "gtp_proxy_last_error": ([_P], C.c_char_p),
+        "gtp_proxy_get_stream": ([_P], _P),
+        "gtp_proxy_set_stream": ([_P, _P], i32),
+        "gtp_proxy_n_param": ([_P], i64),
+        "gtp_proxy_set_training_data": ([_P, _P, _P, i64], i32),
+        "gtp_proxy_get_norm": ([_P, _P, _P], i32),
+        "gtp_proxy_train": ([_P, i32, _P], i32),
+        "gtp_proxy_compute_grads": ([_P, _P, C.POINTER(f)], i32),
+        "gtp_proxy_adam_step": ([_P], i32),
+        "gtp_proxy_get_params": ([_P, _P], i32),
+        "gtp_proxy_set_params": ([_P, _P], i32),
+        "gtp_proxy_get_grads": ([_P, _P], i32),
+        "gtp_proxy_predict": ([_P, _P, i64, _P], i32),
+        "gtp_toggle_bits": ([_P, _P, _P, i32, i64, i64, i64, _P, i64, _P], i32),
+        "gtp_net_toggle_stats": ([_P, _P, i32, i64, i64, i64, _P, _P, _P, _P], i32),
+        "gtp_bf16_gemm": ([_P, i64, _P, i64, i64, i64, i64, _P, i32, _P, i64, _P], i32),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res

@@ -16,7 +16,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgtpb200.so")
 SYNTH_LIB = os.path.join(LIBDIR, "libgtpb200_synth.so")
 
-ENGINE_SOURCES = ["abi.cu", "power_kernel.cu", "pack.cpp"]
+ENGINE_SOURCES = ["abi.cu", "power_kernel.cu", "pack.cpp", "umma_gemm.cu", "proxy.cu"]
 SYNTH_SOURCES = ["synth.cpp"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -29,12 +29,29 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def cutlass_include() -> str:
+    """CuTe/CUTLASS header tree (descriptor unions for tcgen05 operands).
+    Taken from an installed package that vendors it; not linked, headers only."""
+    import importlib.util
+    cands = [os.environ.get("CUTLASS_INCLUDE", "")]
+    for pkg, sub in (("flashinfer", ("data", "cutlass", "include")),
+                     ("tilelang", ("3rdparty", "cutlass", "include"))):
+        spec = importlib.util.find_spec(pkg)
+        if spec is not None and spec.submodule_search_locations:
+            cands.append(os.path.join(spec.submodule_search_locations[0], *sub))
+    for c in cands:
+        if c and os.path.exists(os.path.join(c, "cute", "arch", "mma_sm100_desc.hpp")):
+            return c
+    raise RuntimeError("CuTe headers (cute/arch/mma_sm100_desc.hpp) not found; set CUTLASS_INCLUDE")
+
+
 def _newer(target: str, sources: list[str]) -> bool:
     if not os.path.exists(target):
         return True
     t = os.path.getmtime(target)
     deps = sources + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(os.path.dirname(HERE), "include", "gtpb200.h"))
+    incdir = os.path.join(os.path.dirname(HERE), "include")
+    deps += [os.path.join(incdir, f) for f in os.listdir(incdir) if f.endswith(".h")]
     return any(os.path.getmtime(s) > t for s in deps if os.path.exists(s))
 
 
@@ -43,7 +60,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, f) for f in ENGINE_SOURCES]
     if not force and not _newer(LIB, srcs):
         return LIB
-    cmd = [nvcc(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared",
+    cmd = [nvcc(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-I", cutlass_include(),
            "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
            "-o", LIB, *srcs, "-lpthread"]
     if verbose:

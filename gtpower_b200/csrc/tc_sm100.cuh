@@ -1,0 +1,162 @@
+// tc_sm100.cuh — sm_100a building blocks for the proxy network's GEMMs:
+// mbarriers with bounded waits, 2-D TMA tile loads, TMEM allocation,
+// tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator), tcgen05.commit
+// and tcgen05.ld. Hand-written inline PTX; the shared-memory and instruction
+// descriptors are filled through CuTe's sm100 descriptor unions so that the
+// field layout is the one CUTLASS uses.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cute/arch/mma_sm100_desc.hpp>
+
+namespace gtpb {
+namespace tc {
+
+// Longest a single wait may spin before the kernel gives up, in SM clock
+// cycles (about one second at 2 GHz).
+constexpr long long kSpinLimit = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes initialised barriers visible to the async proxy (TMA, tcgen05).
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete. Returns false when
+// `abort` (shared, may be null) becomes non-zero or the spin limit passes.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (abort != nullptr && *abort) return false;
+    if (clock64() - t0 > kSpinLimit) return false;
+  }
+  return true;
+}
+
+// 2-D tiled TMA load of one box into shared memory, completing `bar`'s
+// transaction count. x is the inner (contiguous) coordinate in elements.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// --- TMEM -----------------------------------------------------------------
+// Whole-warp operations.
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// --- descriptors ----------------------------------------------------------
+// K-major operand without swizzle: 8-row x 16-byte core matrices; `sbo` is
+// the byte distance between core matrices adjacent in M/N (8-row groups),
+// `lbo` the distance between the two core matrices adjacent in K.
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  cute::UMMA::SmemDescriptor d;
+  d.start_address_ = static_cast<uint16_t>((saddr >> 4) & 0x3FFF);
+  d.leading_byte_offset_ = static_cast<uint16_t>((lbo >> 4) & 0x3FFF);
+  d.stride_byte_offset_ = static_cast<uint16_t>((sbo >> 4) & 0x3FFF);
+  d.version_ = 1;
+  d.base_offset_ = 0;
+  d.lbo_mode_ = 0;
+  d.layout_type_ = static_cast<uint8_t>(cute::UMMA::LayoutType::SWIZZLE_NONE);
+  return d.desc_;
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major.
+__host__ __device__ inline uint32_t instr_desc_bf16(int m, int n) {
+  cute::UMMA::InstrDescriptor d;
+  d.desc_ = 0;
+  d.c_format_ = static_cast<uint8_t>(cute::UMMA::CFormat::F32);
+  d.a_format_ = static_cast<uint8_t>(cute::UMMA::F16F32Format::BF16);
+  d.b_format_ = static_cast<uint8_t>(cute::UMMA::F16F32Format::BF16);
+  d.a_major_ = 0;
+  d.b_major_ = 0;
+  d.n_dim_ = static_cast<uint8_t>(n >> 3);
+  d.m_dim_ = static_cast<uint8_t>(m >> 4);
+  return d.desc_;
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T for one K=16 step; issued by one thread.
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+      : "memory");
+}
+
+// Arrives on `bar` once every tcgen05.mma this thread issued so far is done.
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Each thread of the warp reads 16 consecutive FP32 columns of its TMEM
+// lane (lane = warp's lane quarter + laneid).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace tc
+}  // namespace gtpb

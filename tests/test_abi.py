@@ -14,9 +14,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    hdr = open(os.path.join(ROOT, "include", "gtpb200.h")).read()
+    inc = os.path.join(ROOT, "include")
+    hdr = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
-    return sorted(set(re.findall(r"\b(gtp_[a-z_]+)\s*\(", hdr)))
+    return sorted(set(re.findall(r"\b(gtp_[a-z0-9_]+)\s*\(", hdr)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -32,9 +33,11 @@ def test_struct_layout_matches_c_compiler(tmp_path):
     # the ctypes mirror must agree with the C compiler's layout of the header
     import subprocess
     names = ["gtp_table", "gtp_when", "gtp_internal_power", "gtp_leakage_power",
-             "gtp_cell_type", "gtp_design", "gtp_events", "gtp_config", "gtp_counts"]
+             "gtp_cell_type", "gtp_design", "gtp_events", "gtp_config", "gtp_counts",
+             "gtp_proxy_config"]
     src = tmp_path / "sz.c"
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtpb200.h"', "int main(void){"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtpb200.h"',
+             '#include "gtpb200_proxy.h"', "int main(void){"]
     for n in names:
         lines.append(f'printf("{n} %zu\\n", sizeof({n}));')
     for f, _ in _abi.gtp_design._fields_:
