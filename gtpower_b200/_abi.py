@@ -108,6 +108,7 @@ EXPORTED = sorted([
     "gtp_ticks_per_cycle", "gtp_reset", "gtp_push_events", "gtp_push_events_device",
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
     "gtp_evaluate_noalloc", "gtp_pack_values",
+    "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
     "gtp_proxy_get_stream", "gtp_proxy_set_stream", "gtp_proxy_n_param",
     "gtp_proxy_set_training_data", "gtp_proxy_get_norm", "gtp_proxy_train",
@@ -164,6 +165,12 @@ def lib() -> C.CDLL:
     L.gtp_evaluate_noalloc.restype = C.c_int32
     L.gtp_pack_values.argtypes = [_P, C.c_int64, _P]
     L.gtp_pack_values.restype = None
+    L.gtp_set_cycle_groups.argtypes = [C.c_void_p, _P, C.c_int32]
+    L.gtp_set_cycle_groups.restype = C.c_int32
+    L.gtp_n_cycle_groups.argtypes = [C.c_void_p]
+    L.gtp_n_cycle_groups.restype = C.c_int32
+    L.gtp_fetch_cycle_groups.argtypes = [C.c_void_p, _P]
+    L.gtp_fetch_cycle_groups.restype = C.c_int32
     _bind_proxy(L)
     _lib = L
     return L

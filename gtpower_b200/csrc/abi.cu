@@ -57,6 +57,12 @@ struct gtp_ctx {
   double fx_dyn = 0, fx_leak = 0;
   int64_t last_t_hi = 0;
   bool any_window = false;
+  // per-cycle waveforms by cell group (gtp_set_cycle_groups)
+  int32_t n_cgroup = 0;
+  int32_t* d_cgroup = nullptr;
+  unsigned long long* d_cyc_acc_g = nullptr;
+  float* d_cycle5_g = nullptr;
+  unsigned long long* d_leak_tmp_g = nullptr;
 };
 
 namespace {
@@ -94,7 +100,8 @@ void free_all(gtp_ctx* c) {
                   c->d_ev_t, c->d_net_base, c->d_ev_v, c->d_cell_acc, c->d_cyc_acc,
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
-                  c->d_keys_out, c->d_order_work, c->d_sort_temp};
+                  c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g,
+                  c->d_cycle5_g, c->d_leak_tmp_g};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -143,14 +150,17 @@ KParams make_params(gtp_ctx* c) {
   k.cnt_cyc = c->d_cnt_cyc;
   k.n_cell = P.n_cell;
   k.status = c->d_status;
+  k.cell_cgroup = c->n_cgroup > 0 ? c->d_cgroup : nullptr;
+  k.n_cgroup = c->n_cgroup;
+  k.cyc_acc_g = c->n_cgroup > 0 ? c->d_cyc_acc_g : nullptr;
   return k;
 }
 
 // Largest cycle tile whose shared memory (bins with counters, event
 // buffers, tables) stays within 227 KB.
-int64_t max_cycles_per_tile(int threads) {
+int64_t max_cycles_per_tile(int threads, int bin_sets) {
   const int64_t budget = 227 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4));
-  return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (kNumCycAcc * 8 + 8)));
+  return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (bin_sets * kNumCycAcc * 8 + 8)));
 }
 
 gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
@@ -160,10 +170,6 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   if (t_lo < 0) { c->err = "t_lo must be >= 0"; return GTP_EINVAL; }
   if (c->any_window && t_lo < c->last_t_hi) {
     c->err = "windows must be pushed in time order without overlap";
-    return GTP_ESTATE;
-  }
-  if (!c->any_window && t_lo != 0) {
-    c->err = "the first window must start at tick 0";
     return GTP_ESTATE;
   }
   const Packed& P = c->P;
@@ -187,7 +193,8 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   // bins + event buffers + tables within 227 KB of shared memory; tile span
   // (ct+1)*tpc within 2^31 ticks, as the walk holds times as 32-bit offsets
   // from the tile start
-  const int64_t max_ct = std::min<int64_t>(max_cycles_per_tile(threads_), (int64_t(INT32_MAX) / P.tpc) - 1);
+  const int64_t max_ct = std::min<int64_t>(max_cycles_per_tile(threads_, c->n_cgroup > 0 ? 2 : 1),
+                                           (int64_t(INT32_MAX) / P.tpc) - 1);
   ct = std::min(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);  // grid.y limit
   if (ct > max_ct || ct < 1) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
@@ -319,9 +326,10 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     }
     if (e != cudaSuccess) goto cuda_err;
   }
-  // fixed-point scales: dynamic energies bounded by max|E| * 2^36 events,
-  // leakage bins by max|leak| * period * 4 * (n_cell + 1)
-  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 36));
+  // fixed-point scales: a per-cycle dynamic bin holds at most 2^30 events of
+  // max|E| (resolution max|E| * 2^-32), leakage bins max|leak| * period * 4 *
+  // (n_cell + 1)
+  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 30));
   c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * 4.0 *
                                  (static_cast<double>(P.n_cell) + 1.0));
   if (gtp_reset(c) != GTP_OK) { set_err(c->err); free_all(c); delete c; return GTP_ECUDA; }
@@ -361,6 +369,8 @@ gtp_status gtp_reset(gtp_ctx* c) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cell, 0, sizeof(uint32_t) * 4 * nc, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cyc, 0, sizeof(unsigned long long) * 2 * ny, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
+  if (e == cudaSuccess && c->n_cgroup > 0)
+    e = cudaMemsetAsync(c->d_cyc_acc_g, 0, sizeof(unsigned long long) * kNumCycAcc * ny * c->n_cgroup, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "reset");
   c->any_window = false;
   c->last_t_hi = 0;
@@ -440,7 +450,7 @@ gtp_status gtp_finalize(gtp_ctx* c) {
   if (!c) return GTP_EINVAL;
   KParams k = make_params(c);
   cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
-                                  c->d_leak_tmp, c->stream);
+                                  c->d_leak_tmp, c->stream, c->d_cycle5_g, c->d_leak_tmp_g);
   if (e != cudaSuccess) return cuda_fail(c, e, "finalize");
   return GTP_OK;
 }
@@ -462,7 +472,7 @@ gtp_status gtp_fetch(gtp_ctx* c, float* cell5, float* cycle5, double* totals, do
   if (st != GTP_OK) return st;
   KParams k = make_params(c);
   cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
-                                  c->d_leak_tmp, c->stream);
+                                  c->d_leak_tmp, c->stream, c->d_cycle5_g, c->d_leak_tmp_g);
   if (e != cudaSuccess) return cuda_fail(c, e, "finalize");
   const Packed& P = c->P;
   const int64_t np = P.n_period;
@@ -498,6 +508,93 @@ gtp_status gtp_fetch(gtp_ctx* c, float* cell5, float* cycle5, double* totals, do
     }
     counts->dropped = static_cast<int64_t>(cyc_cnt[np] + cyc_cnt[np + 1 + np]);
   }
+  return GTP_OK;
+}
+
+gtp_status gtp_set_cycle_groups(gtp_ctx* c, const int32_t* cell_group, int32_t n_group) {
+  if (!c) return GTP_EINVAL;
+  if (c->any_window) {
+    c->err = "gtp_set_cycle_groups: call before the first window (or after gtp_reset)";
+    return GTP_ESTATE;
+  }
+  const Packed& P = c->P;
+  const int32_t nc = P.n_cell;
+  if (n_group < 0 || n_group > kMaxCycleGroups || (n_group > 0 && !cell_group)) {
+    c->err = "gtp_set_cycle_groups: n_group must be in [0, " + std::to_string(kMaxCycleGroups) + "]";
+    return GTP_EINVAL;
+  }
+  for (int32_t i = 0; i < nc && n_group > 0; ++i)
+    if (cell_group[i] < 0 || cell_group[i] >= n_group) {
+      c->err = "gtp_set_cycle_groups: cell " + std::to_string(i) + " has group out of range";
+      return GTP_EINVAL;
+    }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+  void* old[] = {c->d_cgroup, c->d_cyc_acc_g, c->d_cycle5_g, c->d_leak_tmp_g};
+  for (void* q : old)
+    if (q) cudaFree(q);
+  c->d_cgroup = nullptr;
+  c->d_cyc_acc_g = nullptr;
+  c->d_cycle5_g = nullptr;
+  c->d_leak_tmp_g = nullptr;
+  c->n_cgroup = 0;
+  // base walk order: by pin bucket, then (with groups) by group, then as packed
+  std::vector<int32_t> order = P.order;
+  if (n_group > 0) {
+    for (int b = 0; b < 3; ++b)
+      std::stable_sort(order.begin() + P.bucket_begin[b], order.begin() + P.bucket_begin[b + 1],
+                       [&](int32_t x, int32_t y) { return cell_group[x] < cell_group[y]; });
+  }
+  if (nc > 0) {
+    e = cudaMemcpyAsync(c->d_order, order.data(), sizeof(int32_t) * nc, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "walk order upload");
+  }
+  if (n_group == 0) return GTP_OK;
+  const size_t ny = static_cast<size_t>(P.n_period + 1);
+  const size_t np = static_cast<size_t>(std::max<int64_t>(1, P.n_period));
+  e = cudaMalloc(&c->d_cgroup, sizeof(int32_t) * std::max<int32_t>(1, nc));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_cyc_acc_g, sizeof(unsigned long long) * kNumCycAcc * ny * n_group);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_cycle5_g, sizeof(float) * 5 * np * n_group);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_leak_tmp_g, sizeof(unsigned long long) * np * n_group);
+  if (e == cudaSuccess && nc > 0)
+    e = cudaMemcpyAsync(c->d_cgroup, cell_group, sizeof(int32_t) * nc, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(c->d_cyc_acc_g, 0, sizeof(unsigned long long) * kNumCycAcc * ny * n_group, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    void* fr[] = {c->d_cgroup, c->d_cyc_acc_g, c->d_cycle5_g, c->d_leak_tmp_g};
+    for (void* q : fr)
+      if (q) cudaFree(q);
+    c->d_cgroup = nullptr;
+    c->d_cyc_acc_g = nullptr;
+    c->d_cycle5_g = nullptr;
+    c->d_leak_tmp_g = nullptr;
+    return e == cudaErrorMemoryAllocation ? GTP_ENOMEM : cuda_fail(c, e, "cycle groups");
+  }
+  c->n_cgroup = n_group;
+  return GTP_OK;
+}
+
+int32_t gtp_n_cycle_groups(const gtp_ctx* c) { return c ? c->n_cgroup : 0; }
+
+gtp_status gtp_fetch_cycle_groups(gtp_ctx* c, float* cycle5_groups) {
+  if (!c || !cycle5_groups) return GTP_EINVAL;
+  if (c->n_cgroup <= 0) {
+    c->err = "gtp_fetch_cycle_groups: no cycle groups set";
+    return GTP_ESTATE;
+  }
+  gtp_status st = check_status(c);
+  if (st != GTP_OK) return st;
+  KParams k = make_params(c);
+  cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg, c->d_leak_tmp,
+                                  c->stream, c->d_cycle5_g, c->d_leak_tmp_g);
+  const int64_t np = c->P.n_period;
+  if (e == cudaSuccess && np > 0)
+    e = cudaMemcpyAsync(cycle5_groups, c->d_cycle5_g, sizeof(float) * 5 * np * c->n_cgroup,
+                        cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "fetch cycle groups");
   return GTP_OK;
 }
 
@@ -603,6 +700,9 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   k.cyc_acc = reinterpret_cast<unsigned long long*>(s + off_cyc);
   k.cnt_cell = nullptr;
   k.cnt_cyc = nullptr;
+  k.cell_cgroup = nullptr;  // no per-group waveforms on this path
+  k.cyc_acc_g = nullptr;
+  k.n_cgroup = 0;
   k.net_off = ev->net_off;
   k.ev_t = ev->time;
   k.ev_v = ev->value_packed;
@@ -616,7 +716,7 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   int64_t ct = c->cfg.cycles_per_tile > 0 ? c->cfg.cycles_per_tile : 512;
   ct = std::min<int64_t>(ct, n_cyc);
   const int64_t max_ct = std::min<int64_t>(
-      max_cycles_per_tile(c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256),
+      max_cycles_per_tile(c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256, 1),
       (int64_t(INT32_MAX) / P.tpc) - 1);
   ct = std::min<int64_t>(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);

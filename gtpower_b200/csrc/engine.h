@@ -162,9 +162,16 @@ struct KParams {
   unsigned long long* cnt_cyc;      // [2][n_period+1]
   int32_t n_cell;
   int32_t* status;                  // error bits
+  // per-cycle accumulators by cell group (optional)
+  const int32_t* cell_cgroup;       // [n_cell] group of each cell, or null
+  int32_t n_cgroup;
+  unsigned long long* cyc_acc_g;    // [n_cgroup][6][n_period+1]
 };
 
 // status bits set by the kernel
+// largest number of per-cycle cell groups (sort keys hold the group in 18 bits)
+constexpr int32_t kMaxCycleGroups = 65536;
+
 constexpr int32_t kErrNetRange = 1;
 constexpr int32_t kErrTimeOrder = 2;
 constexpr int32_t kErrTimeRange = 4;
@@ -173,11 +180,13 @@ constexpr int32_t kErrContext = 8;
 // Launches the walk over one bucket of cells. shared-memory bytes computed inside.
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
                               cudaStream_t stream);
+// bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group.
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
-                             size_t tab_bytes);
+                             size_t tab_bytes, int bin_sets = 1);
 
 // Walk order for one window: cells stay grouped by pin bucket and, within a
-// bucket, are sorted by the number of events on their pins (descending).
+// bucket, by cell group when groups are set, and are sorted by the number of
+// events on their pins (descending) within that.
 size_t work_sort_temp_bytes(int32_t n_cell);
 cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int32_t n_cell,
                                const int32_t* bucket_begin, unsigned long long* keys_in,
@@ -185,8 +194,11 @@ cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int3
                                size_t temp_bytes, cudaStream_t stream);
 
 // Finalize kernels: per-cell floats, totals/groups, per-cycle floats.
+// With d_cycle5_g (and p.cyc_acc_g), also the per-group per-cycle floats
+// [n_cgroup][5][n_period], using d_leak_tmp_g [n_cgroup][n_period].
 cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,
                             float* d_cycle5, double* d_totals_groups,
-                            unsigned long long* d_leak_prefix_tmp, cudaStream_t stream);
+                            unsigned long long* d_leak_prefix_tmp, cudaStream_t stream,
+                            float* d_cycle5_g = nullptr, unsigned long long* d_leak_tmp_g = nullptr);
 
 }  // namespace gtpb

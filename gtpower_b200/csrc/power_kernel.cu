@@ -109,10 +109,12 @@ __device__ __forceinline__ T sel(const T (&a)[N], int i) {
 }
 
 struct Bins {
-  unsigned long long* s;   // [6][ct] fixed-point energies
+  unsigned long long* s;   // [sets][6][ct] fixed-point energies
   uint32_t* sc;            // [2][ct] counts
   int64_t c_lo;            // first cycle of the tile
   int64_t ct;              // cycles in the tile
+  int64_t off;             // this cell's bin set (set * 6 * ct), -1: add to global memory
+  int32_t g;               // this cell's group when per-cycle groups are kept
 };
 
 // per-cycle accumulator slots
@@ -124,11 +126,13 @@ __device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, 
                                         unsigned long long x) {
   if (x == 0ull) return;
   const int64_t k = c - b.c_lo;
-  if (k >= 0 && k < b.ct) {
-    atomicAdd(b.s + q * b.ct + k, x);
+  if (k >= 0 && k < b.ct && b.off >= 0) {
+    atomicAdd(b.s + b.off + q * b.ct + k, x);
   } else {
     const int64_t cc = c < 0 ? p.n_period : (c < p.n_period ? c : p.n_period);
     atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
+    if (p.cyc_acc_g)
+      atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(b.g) * kNumCycAcc + q) * (p.n_period + 1) + cc, x);
   }
 }
 
@@ -222,20 +226,24 @@ template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const KParams p) {
   extern __shared__ unsigned long long smem[];
   const int64_t ct = p.cycles_per_tile;
+  // per-cycle groups: two bin sets, for the block's first group and the next
+  const int nset = p.cell_cgroup ? 2 : 1;
   Bins bins;
   bins.s = smem;
-  bins.sc = reinterpret_cast<uint32_t*>(smem + kNumCycAcc * ct);
+  bins.sc = reinterpret_cast<uint32_t*>(smem + nset * kNumCycAcc * ct);
+  bins.off = 0;
+  bins.g = 0;
   const int tile = blockIdx.y;
   bins.c_lo = p.cyc0 + static_cast<int64_t>(tile) * ct;
   bins.ct = ct;
-  for (int64_t k = threadIdx.x; k < kNumCycAcc * ct; k += blockDim.x) smem[k] = 0ull;
+  for (int64_t k = threadIdx.x; k < nset * kNumCycAcc * ct; k += blockDim.x) smem[k] = 0ull;
   if (COUNTS)
     for (int64_t k = threadIdx.x; k < 2 * ct; k += blockDim.x) bins.sc[k] = 0u;
   // RING: per-thread event buffers [pin][slot][thread] of times - T0, then
   // the per-type energy-selection and leakage tables when they fit
   constexpr bool RING = FAST && WALK_USE_RING;
   constexpr bool STAGE = FAST && WALK_STAGE_INST;
-  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + kNumCycAcc * ct + (COUNTS ? ct : 0));
+  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + nset * kNumCycAcc * ct + (COUNTS ? ct : 0));
   const int nt_blk = blockDim.x;
   const int16_t* fast_tab = p.fast_tab;
   const float* leak_pool = p.leak_pool;
@@ -263,9 +271,17 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
 
   const int32_t g_begin = p.order_begin + blockIdx.x * p.gates_per_block;
   const int32_t g_end = min(p.order_end, g_begin + p.gates_per_block);
+  // cells are ordered by group within a bucket: the block's first cell has
+  // its smallest group
+  const int32_t g_first = p.cell_cgroup ? __ldg(p.cell_cgroup + __ldg(p.order + g_begin)) : 0;
 
   for (int32_t gi = g_begin + threadIdx.x; gi < g_end; gi += blockDim.x) {
     const int32_t cell = __ldg(p.order + gi);
+    if (p.cell_cgroup) {
+      bins.g = __ldg(p.cell_cgroup + cell);
+      const int32_t set = bins.g - g_first;
+      bins.off = (set == 0 || set == 1) ? static_cast<int64_t>(set) * kNumCycAcc * ct : -1;
+    }
     const int32_t p0 = __ldg(p.cell_pin_off + cell);
     const int32_t type = __ldg(p.cell_type + cell);
     const DevType ty = p.types[type];
@@ -684,8 +700,13 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
     const int64_t cc = c < p.n_period ? c : p.n_period;
 #pragma unroll
     for (int q = 0; q < kNumCycAcc; ++q) {
-      const unsigned long long x = smem[q * ct + k];
-      if (x) atomicAdd(p.cyc_acc + q * stride + cc, x);
+      const unsigned long long x0 = smem[q * ct + k];
+      const unsigned long long x1 = nset == 2 ? smem[(kNumCycAcc + q) * ct + k] : 0ull;
+      if (x0 + x1) atomicAdd(p.cyc_acc + q * stride + cc, x0 + x1);
+      if (p.cyc_acc_g) {
+        if (x0) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g_first) * kNumCycAcc + q) * stride + cc, x0);
+        if (x1) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g_first + 1) * kNumCycAcc + q) * stride + cc, x1);
+      }
     }
     if (COUNTS) {
       const uint32_t a = bins.sc[k], b2 = bins.sc[ct + k];
@@ -711,7 +732,12 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
   const unsigned long long bucket = k >= b2 ? 2ull : (k >= b1 ? 1ull : 0ull);
   const unsigned long long cap = (1ull << 40) - 1;
   const unsigned long long wc = w < 0 ? 0ull : (static_cast<unsigned long long>(w) > cap ? cap : static_cast<unsigned long long>(w));
-  keys[k] = (bucket << 40) | (cap - wc);
+  // bits [0,40): inverted work; then the bucket, or with per-cycle groups
+  // the cell group in [40,58) and the bucket in [58,60)
+  if (p.cell_cgroup)
+    keys[k] = (bucket << 58) | (static_cast<unsigned long long>(p.cell_cgroup[cell]) << 40) | (cap - wc);
+  else
+    keys[k] = (bucket << 40) | (cap - wc);
 }
 
 }  // namespace
@@ -721,7 +747,7 @@ size_t work_sort_temp_bytes(int32_t n_cell) {
   cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const unsigned long long*>(nullptr),
                                   static_cast<unsigned long long*>(nullptr),
                                   static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
-                                  n_cell, 0, 42);
+                                  n_cell, 0, 60);
   return bytes;
 }
 
@@ -734,8 +760,9 @@ cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int3
                                                              bucket_begin[2], keys_in);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  const int end_bit = p.cell_cgroup ? 60 : 42;
   return cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, base_order, order_out,
-                                         n_cell, 0, 42, stream);
+                                         n_cell, 0, end_bit, stream);
 }
 
 namespace {
@@ -780,11 +807,16 @@ __global__ void finalize_cells(const KParams p, const uint8_t* __restrict__ grou
 // One block: prefix-sums the leakage level differences and converts the
 // fixed-point per-cycle energies to watts. The level of cycle c covers the
 // part of the cycle before time_max.
-__global__ void finalize_cycles(const KParams p, float* __restrict__ cycle5,
-                                unsigned long long* __restrict__ leak_tmp) {
+// Block b handles accumulator set b: acc_base + b * 6 * (n_period + 1), with
+// its outputs at cycle5_base + b * 5 * n_period.
+__global__ void finalize_cycles(const KParams p, const unsigned long long* __restrict__ acc_base,
+                                float* __restrict__ cycle5_base,
+                                unsigned long long* __restrict__ leak_tmp_base) {
   const int64_t np = p.n_period;
   const int64_t stride = np + 1;
-  const unsigned long long* acc = p.cyc_acc;
+  const unsigned long long* acc = acc_base + static_cast<int64_t>(blockIdx.x) * kNumCycAcc * stride;
+  float* cycle5 = cycle5_base + static_cast<int64_t>(blockIdx.x) * 5 * np;
+  unsigned long long* leak_tmp = leak_tmp_base + static_cast<int64_t>(blockIdx.x) * np;
   __shared__ unsigned long long carry_s;
   __shared__ unsigned long long warp_sums[32];
   if (threadIdx.x == 0) carry_s = 0;
@@ -843,7 +875,8 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   size_t tabs = (FAST && p.tabs_in_smem) ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16 : 0;
   if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
   const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads,
-                                            (FAST && WALK_USE_RING) ? MAXP : 0, tabs);
+                                            (FAST && WALK_USE_RING) ? MAXP : 0, tabs,
+                                            p.cell_cgroup ? 2 : 1);
   auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -856,8 +889,8 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
 }  // namespace
 
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
-                             size_t tab_bytes) {
-  return static_cast<size_t>(cycles_per_tile) * (kNumCycAcc * 8 + (counts ? 8 : 0)) +
+                             size_t tab_bytes, int bin_sets) {
+  return static_cast<size_t>(cycles_per_tile) * (bin_sets * kNumCycAcc * 8 + (counts ? 8 : 0)) +
          static_cast<size_t>(ring_pins) * kRing * threads * 4 + tab_bytes;
 }
 
@@ -884,7 +917,7 @@ cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int t
 
 cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,
                             float* d_cycle5, double* d_tg, unsigned long long* d_leak_tmp,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, float* d_cycle5_g, unsigned long long* d_leak_tmp_g) {
   cudaError_t e = cudaMemsetAsync(d_tg, 0, sizeof(double) * (GTP_N_GROUP + 1) * 5, stream);
   if (e != cudaSuccess) return e;
   if (p.n_cell > 0) {
@@ -894,8 +927,12 @@ cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* 
     if (e != cudaSuccess) return e;
   }
   if (p.n_period > 0) {
-    finalize_cycles<<<1, 1024, 0, stream>>>(p, d_cycle5, d_leak_tmp);
+    finalize_cycles<<<1, 1024, 0, stream>>>(p, p.cyc_acc, d_cycle5, d_leak_tmp);
     e = cudaGetLastError();
+    if (e == cudaSuccess && p.cyc_acc_g && d_cycle5_g && d_leak_tmp_g && p.n_cgroup > 0) {
+      finalize_cycles<<<p.n_cgroup, 1024, 0, stream>>>(p, p.cyc_acc_g, d_cycle5_g, d_leak_tmp_g);
+      e = cudaGetLastError();
+    }
   }
   return e;
 }

@@ -16,6 +16,11 @@
 //                     factor ~ lognormal(0, sigma) normalised to mean 1;
 //   mode 2 (phases) : 16-state sticky Markov chain over cycles; each
 //                     (phase, net) pair has its own rate ~ U[lo, hi].
+//   mode 3 (phased units): the same phase chain; nets are split into n_unit
+//                     contiguous id ranges ("units"), each net has a base
+//                     rate u ~ U[lo, hi], and each (phase, unit) pair an
+//                     activity factor a ~ lognormal(-s^2/2, s) (mean 1); the
+//                     toggle probability is min(0.9, u * a).
 // A toggle lands at a uniform offset within the cycle; with probability
 // glitch_p it is followed by a pulse of width w ~ U[w_lo, w_hi] ticks (two
 // extra value flips at +w and +2w, kept inside the cycle). The clock net
@@ -69,8 +74,10 @@ struct TraceParams {
   int32_t mode;
   double lo, hi;             // mode 0 / 2 rate range
   double zipf_alpha, rate_mean, burst_sigma;  // mode 1
-  int32_t n_phase;           // mode 2
-  double p_stay;             // mode 2
+  int32_t n_phase;           // mode 2 / 3
+  double p_stay;             // mode 2 / 3
+  int32_t n_unit;            // mode 3
+  double act_sigma;          // mode 3
   double glitch_p;
   int64_t w_lo, w_hi;
   int32_t clock_net;
@@ -82,10 +89,15 @@ struct Trace {
   std::vector<double> net_rate;     // mode 0/1
   std::vector<uint32_t> rank;       // mode 1
   std::vector<double> burst;        // mode 1: per cycle factor
-  std::vector<uint8_t> phase;       // mode 2: per cycle phase
+  std::vector<uint8_t> phase;       // mode 2 / 3: per cycle phase
+  std::vector<double> act;          // mode 3: [phase][unit] activity factor
   double prob(int32_t net, int64_t c) const {
     if (tp.mode == 0) return net_rate[net];
     if (tp.mode == 1) return std::min(1.0, net_rate[net] * burst[c]);
+    if (tp.mode == 3) {
+      const int64_t u = static_cast<int64_t>(net) * tp.n_unit / tp.n_net;
+      return std::min(0.9, net_rate[net] * act[static_cast<size_t>(phase[c]) * tp.n_unit + u]);
+    }
     const uint64_t h = hash3(tp.seed ^ 0x5A5A, static_cast<uint64_t>(net), phase[c], 77);
     return tp.lo + (tp.hi - tp.lo) * u01(h);
   }
@@ -254,6 +266,8 @@ void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int6
   tp.burst_sigma = burst_sigma; tp.n_phase = n_phase; tp.p_stay = p_stay;
   tp.glitch_p = glitch_p; tp.w_lo = w_lo; tp.w_hi = w_hi; tp.clock_net = clock_net;
   tp.n_net = n_net;
+  tp.n_unit = 1;
+  tp.act_sigma = 0.0;
   Rng rng(seed ^ 0x1234567ull);
   if (mode == 0) {
     tr->net_rate.resize(n_net);
@@ -288,6 +302,28 @@ void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int6
       tr->phase[c] = ph;
     }
   }
+  return tr;
+}
+
+// Mode 3 trace (phased units); see the header comment.
+void* synth_trace_create_phased(int32_t n_net, int32_t clock_net, int64_t n_cycle, int64_t tpc,
+                                uint64_t seed, double lo, double hi, int32_t n_phase, double p_stay,
+                                int32_t n_unit, double act_sigma, double glitch_p, int64_t w_lo,
+                                int64_t w_hi) {
+  if (n_phase < 1 || n_phase > 255 || n_unit < 1 || n_net < 1) return nullptr;
+  // the phase chain exactly as mode 2 draws it
+  Trace* tr = static_cast<Trace*>(synth_trace_create(n_net, clock_net, n_cycle, tpc, seed, 2, lo, hi, 0.0,
+                                                     0.0, 0.0, n_phase, p_stay, glitch_p, w_lo, w_hi));
+  TraceParams& tp = tr->tp;
+  tp.mode = 3;
+  tp.n_unit = std::min(n_unit, n_net);
+  tp.act_sigma = act_sigma;
+  tr->net_rate.resize(n_net);
+  for (int32_t n = 0; n < n_net; ++n)
+    tr->net_rate[n] = lo + (hi - lo) * u01(hash3(seed, n, 0xFFFFFFFFull, 9));
+  tr->act.resize(static_cast<size_t>(n_phase) * tp.n_unit);
+  Rng ar(seed ^ 0xAC71u);
+  for (double& a : tr->act) a = std::exp(act_sigma * ar.normal() - 0.5 * act_sigma * act_sigma);
   return tr;
 }
 

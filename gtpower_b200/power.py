@@ -85,7 +85,7 @@ class B200Power:
 
     def __init__(self, design: Design, *, collect_counts: bool = False, device: int = -1,
                  cycles_per_tile: int = 0, threads_per_block: int = 0, gates_per_block: int = 0,
-                 max_n_pin_for_leakage_power: int = 16):
+                 max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None):
         self.design = design
         L = _abi.lib()
         cfg = _abi.gtp_config()
@@ -96,6 +96,8 @@ class B200Power:
         cfg.n_thread_per_block = threads_per_block
         cfg.gates_per_block = gates_per_block
         cfg.max_n_pin_for_leakage_power = max_n_pin_for_leakage_power
+        if sort_by_work is not None:
+            cfg.sort_by_work = 1 if sort_by_work else 0
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()
@@ -155,6 +157,26 @@ class B200Power:
 
     def sync(self) -> None:
         _abi.check(_abi.lib().gtp_sync(self.ctx), self.ctx)
+
+    # -- per-cycle waveforms by cell group ----------------------------------
+    def set_cycle_groups(self, cell_group: np.ndarray | None, n_group: int = 0) -> None:
+        """Keeps per-cycle waveforms per cell group as well (before the first
+        window). cell_group: int32 [n_cell] in [0, n_group); None turns it off."""
+        if cell_group is None:
+            _abi.check(_abi.lib().gtp_set_cycle_groups(self.ctx, None, 0), self.ctx)
+            return
+        g = np.ascontiguousarray(cell_group, dtype=np.int32)
+        assert g.shape == (self.design.n_cell,)
+        _abi.check(_abi.lib().gtp_set_cycle_groups(self.ctx, g.ctypes.data_as(C.c_void_p), int(n_group)),
+                   self.ctx)
+
+    def fetch_cycle_groups(self) -> np.ndarray:
+        """[n_group, 5, n_period] float32: the cycle5 rows of each group."""
+        L = _abi.lib()
+        ng = int(L.gtp_n_cycle_groups(self.ctx))
+        out = np.zeros((ng, 5, self.n_period), dtype=np.float32)
+        _abi.check(L.gtp_fetch_cycle_groups(self.ctx, out.ctypes.data_as(C.c_void_p)), self.ctx)
+        return out
 
     # -- results ----------------------------------------------------------
     def fetch(self, counts: bool = False) -> Results:

@@ -58,6 +58,10 @@ def synth_lib() -> C.CDLL:
                                          C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int32, C.c_double, C.c_double, C.c_int64,
                                          C.c_int64]
+        L.synth_trace_create_phased.restype = C.c_void_p
+        L.synth_trace_create_phased.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_uint64,
+                                                C.c_double, C.c_double, C.c_int32, C.c_double,
+                                                C.c_int32, C.c_double, C.c_double, C.c_int64, C.c_int64]
         L.synth_trace_free.argtypes = [C.c_void_p]
         L.synth_trace_phase.restype = C.c_int32
         L.synth_trace_phase.argtypes = [C.c_void_p, C.c_int64]
@@ -268,7 +272,7 @@ def flat_design(spec: FlatSpec, cells_path: str = DATA) -> tuple[Design, dict]:
 
 @dataclass
 class TraceSpec:
-    mode: int = 0              # 0 uniform, 1 zipf+burst, 2 markov phases
+    mode: int = 0              # 0 uniform, 1 zipf+burst, 2 markov phases, 3 phased units
     lo: float = 0.05
     hi: float = 0.30
     zipf_alpha: float = 1.2
@@ -276,6 +280,8 @@ class TraceSpec:
     burst_sigma: float = 1.5
     n_phase: int = 16
     p_stay: float = 0.99
+    n_unit: int = 32           # mode 3: contiguous net ranges with per-phase activity
+    act_sigma: float = 0.8     # mode 3: lognormal sigma of the activity factors
     glitch_p: float = 0.05
     w_lo_ticks: int = 5
     w_hi_ticks: int = 100
@@ -292,10 +298,18 @@ class Trace:
         self.n_cycle = info["n_cycle"]
         self.tpc = info["tpc"]
         L = synth_lib()
-        self.h = L.synth_trace_create(self.n_net, info["clock_net"], self.n_cycle, self.tpc, seed,
-                                      spec.mode, spec.lo, spec.hi, spec.zipf_alpha, spec.rate_mean,
-                                      spec.burst_sigma, spec.n_phase, spec.p_stay, spec.glitch_p,
-                                      spec.w_lo_ticks, spec.w_hi_ticks)
+        if spec.mode == 3:
+            self.h = L.synth_trace_create_phased(self.n_net, info["clock_net"], self.n_cycle, self.tpc,
+                                                 seed, spec.lo, spec.hi, spec.n_phase, spec.p_stay,
+                                                 spec.n_unit, spec.act_sigma, spec.glitch_p,
+                                                 spec.w_lo_ticks, spec.w_hi_ticks)
+        else:
+            self.h = L.synth_trace_create(self.n_net, info["clock_net"], self.n_cycle, self.tpc, seed,
+                                          spec.mode, spec.lo, spec.hi, spec.zipf_alpha, spec.rate_mean,
+                                          spec.burst_sigma, spec.n_phase, spec.p_stay, spec.glitch_p,
+                                          spec.w_lo_ticks, spec.w_hi_ticks)
+        if not self.h:
+            raise ValueError("invalid trace parameters")
         self.init = np.empty(self.n_net, dtype=np.uint8)
         L.synth_trace_initial(self.h, _p(self.init))
 

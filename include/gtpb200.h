@@ -241,7 +241,10 @@ int64_t     gtp_ticks_per_cycle(const gtp_ctx* ctx);
 gtp_status  gtp_reset(gtp_ctx* ctx);
 
 /* Copies one window of events from host memory (pinned or pageable) to the
- * device and evaluates it. Windows must come in time order. */
+ * device and evaluates it. Windows must come in time order without overlap.
+ * Gaps are allowed: cycles no window covers keep zero per-cycle power, and
+ * per-cell values then cover the evaluated windows only (a spot check of
+ * selected cycle ranges, e.g. the learned proxy's audit sample). */
 gtp_status  gtp_push_events(gtp_ctx* ctx, const gtp_events* ev);
 
 /* Same, with events already in device memory (time, value_packed, net_off,
@@ -274,6 +277,18 @@ gtp_status  gtp_finalize(gtp_ctx* ctx);
  */
 gtp_status  gtp_fetch(gtp_ctx* ctx, float* cell5, float* cycle5,
                       double* totals, double* groups, gtp_counts* counts);
+
+/* Per-cycle waveforms by cell group. No counterpart in the reference, whose
+ * per-cycle output (cuda_per_cycle_waveform.txt,
+ * include/sta/PowerClass.hh:123-149) covers the whole design only. Used to
+ * label per-block power for the learned proxy (include/gtpb200_proxy.h).
+ * cell_group[i] in [0, n_group) for every cell, n_group <= 65536; n_group = 0
+ * turns grouping off. Call before the first window or after gtp_reset. The
+ * whole-design waveforms of gtp_fetch are unchanged. */
+gtp_status  gtp_set_cycle_groups(gtp_ctx* ctx, const int32_t* cell_group, int32_t n_group);
+int32_t     gtp_n_cycle_groups(const gtp_ctx* ctx);
+/* cycle5_groups [n_group][5][n_period]: per group, the rows of cycle5. */
+gtp_status  gtp_fetch_cycle_groups(gtp_ctx* ctx, float* cycle5_groups);
 
 /* Allocation-free evaluation. No counterpart in the reference.
  *

@@ -84,3 +84,43 @@ def test_streamed_skew_trace(window):
         wins.append(w)
     res = run_engine(d, wins, cycles_per_tile=6)
     compare(res, oracle(d, full))
+
+
+@pytest.mark.parametrize("sort_by_work", [True, False])
+@pytest.mark.parametrize("n_group,layout,gpb", [(4, "blocks", 0), (7, "blocks", 64), (5, "random", 0),
+                                                (500, "random", 0)])
+def test_cycle_groups_match_oracle_on_cell_subsets(n_group, layout, gpb, sort_by_work):
+    """Per-cycle waveforms by cell group equal the oracle restricted to each
+    group's cells; the whole-design waveforms are unchanged. 500 groups over
+    3000 cells make every block span many groups (the global-memory path)."""
+    from gtpower_b200 import B200Power, synth, windows
+    from oracle import oracle as orc
+    from tests.parity import close
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=3000, n_cycle=90, seed=21))
+    ev = synth.Trace(d, info, synth.TraceSpec(glitch_p=0.1), seed=22).full()
+    if layout == "blocks":
+        grp = (np.arange(d.n_cell) * n_group // d.n_cell).astype(np.int32)
+    else:
+        grp = np.random.default_rng(n_group).integers(0, n_group, d.n_cell).astype(np.int32)
+    wins = windows.split(ev, d.ticks_per_cycle, [0, 31, 90])
+    with B200Power(d, gates_per_block=gpb, cycles_per_tile=16, sort_by_work=sort_by_work) as eng:
+        eng.set_cycle_groups(grp, n_group)
+        for w in wins:
+            eng.read_power_activities(w)
+        res = eng.fetch()
+        G = eng.fetch_cycle_groups()
+    full = orc.run(d, ev)
+    close("cycle5", res.cycle5.T, full.cycle5.T)
+    close("totals", res.totals, full.totals)
+    # Per-event energies are FP32 (the reference's float table values), so a
+    # group sum that nearly cancels (negative fall energies) carries FP32
+    # rounding relative to its terms: values below 1e-3 of the whole
+    # design's column maximum are held to 1e-8 of that maximum.
+    scale = np.max(np.abs(full.cycle5.T), axis=0, keepdims=True)
+    for g in sorted(set(grp.tolist()))[:12]:
+        o = orc.run(d, ev, cells=np.nonzero(grp == g)[0])
+        ref = o.cycle5.T
+        tol = 1e-5 * np.maximum(np.abs(ref), 1e-3 * scale)
+        err = np.abs(G[g].T.astype(np.float64) - ref)
+        assert (err <= tol).all(), (g, np.argwhere(err > tol)[:5].tolist())
+    close("sum of groups", G.sum(0).T, full.cycle5.T)
