@@ -156,7 +156,7 @@ def run_proxy(args):
     tspec = synth.TraceSpec(mode=3, lo=0.02, hi=0.12, n_phase=16, p_stay=0.99, n_unit=32, act_sigma=1.0,
                             glitch_p=0.05)
     trace = synth.Trace(design, info, tspec, seed=20261203 + 4)
-    wins = pf.upload_trace(trace, args.proxy_window)
+    wins = pf.generate_on_device(trace, args.proxy_window)
     n_event = sum(w.n_event for w in wins)
     gen_s = time.time() - t0
     print(f"# trace: {n_event} events in {len(wins)} windows, {gen_s:.1f} s", file=sys.stderr, flush=True)

@@ -15,9 +15,11 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgtpb200.so")
 SYNTH_LIB = os.path.join(LIBDIR, "libgtpb200_synth.so")
+SYNTHDEV_LIB = os.path.join(LIBDIR, "libgtpb200_synthdev.so")
 
 ENGINE_SOURCES = ["abi.cu", "power_kernel.cu", "pack.cpp", "umma_gemm.cu", "proxy.cu"]
 SYNTH_SOURCES = ["synth.cpp"]
+SYNTHDEV_SOURCES = ["synth_dev.cu"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -80,9 +82,22 @@ def build_synth(force: bool = False) -> str:
     return SYNTH_LIB
 
 
+def build_synthdev(force: bool = False) -> str:
+    """The synthetic-trace generator on the GPU (sm_100a)."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    srcs = [os.path.join(CSRC, f) for f in SYNTHDEV_SOURCES]
+    if not force and not _newer(SYNTHDEV_LIB, srcs):
+        return SYNTHDEV_LIB
+    cmd = [nvcc(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+           "-o", SYNTHDEV_LIB, *srcs]
+    subprocess.run(cmd, check=True)
+    return SYNTHDEV_LIB
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_engine(force=force, verbose=verbose)
     build_synth(force=force)
+    build_synthdev(force=force)
 
 
 if __name__ == "__main__":

@@ -33,19 +33,13 @@
 #include <thread>
 #include <vector>
 
+#include "synth_rules.h"
+
 namespace {
 
-inline uint64_t splitmix(uint64_t x) {
-  x += 0x9E3779B97F4A7C15ull;
-  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-  return x ^ (x >> 31);
-}
-inline uint64_t hash3(uint64_t seed, uint64_t a, uint64_t b, uint64_t c) {
-  return splitmix(splitmix(splitmix(seed ^ (a * 0xD6E8FEB86659FD93ull)) ^ (b + 0x632BE59BD9B4E019ull)) ^
-                  (c * 0x9E3779B97F4A7C15ull + 1));
-}
-inline double u01(uint64_t h) { return (h >> 11) * (1.0 / 9007199254740992.0); }
+using gtpb::syn::hash3;
+using gtpb::syn::splitmix;
+using gtpb::syn::u01;
 
 struct Rng {  // sequential generator for netlist construction
   uint64_t s;
@@ -86,55 +80,35 @@ struct TraceParams {
 
 struct Trace {
   TraceParams tp;
-  std::vector<double> net_rate;     // mode 0/1
+  std::vector<double> net_rate;     // mode 0/1/3
   std::vector<uint32_t> rank;       // mode 1
   std::vector<double> burst;        // mode 1: per cycle factor
   std::vector<uint8_t> phase;       // mode 2 / 3: per cycle phase
   std::vector<double> act;          // mode 3: [phase][unit] activity factor
-  double prob(int32_t net, int64_t c) const {
-    if (tp.mode == 0) return net_rate[net];
-    if (tp.mode == 1) return std::min(1.0, net_rate[net] * burst[c]);
-    if (tp.mode == 3) {
-      const int64_t u = static_cast<int64_t>(net) * tp.n_unit / tp.n_net;
-      return std::min(0.9, net_rate[net] * act[static_cast<size_t>(phase[c]) * tp.n_unit + u]);
-    }
-    const uint64_t h = hash3(tp.seed ^ 0x5A5A, static_cast<uint64_t>(net), phase[c], 77);
-    return tp.lo + (tp.hi - tp.lo) * u01(h);
+  gtpb::syn::Rules rules{};         // view of the above, set once the tables are final
+  void set_rules() {
+    rules.mode = tp.mode;
+    rules.clock_net = tp.clock_net;
+    rules.n_net = tp.n_net;
+    rules.n_unit = tp.n_unit;
+    rules.n_cycle = tp.n_cycle;
+    rules.tpc = tp.tpc;
+    rules.seed = tp.seed;
+    rules.lo = tp.lo;
+    rules.hi = tp.hi;
+    rules.glitch_p = tp.glitch_p;
+    rules.w_lo = tp.w_lo;
+    rules.w_hi = tp.w_hi;
+    rules.net_rate = net_rate.empty() ? nullptr : net_rate.data();
+    rules.burst = burst.empty() ? nullptr : burst.data();
+    rules.phase = phase.empty() ? nullptr : phase.data();
+    rules.act = act.empty() ? nullptr : act.data();
   }
 };
 
-// Events of one net in cycle c; writes up to 3 (time, flip) pairs.
+// Events of one net in cycle c; writes up to 3 ticks.
 inline int cycle_events(const Trace& tr, int32_t net, int64_t c, int64_t* t) {
-  const TraceParams& tp = tr.tp;
-  const int64_t base = c * tp.tpc;
-  if (net == tp.clock_net) {  // falls at the cycle boundary, rises mid-cycle
-    if (c == 0) {
-      t[0] = base + tp.tpc / 2;
-      return 1;
-    }
-    t[0] = base;
-    t[1] = base + tp.tpc / 2;
-    return 2;
-  }
-  const uint64_t h = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 1);
-  if (u01(h) >= tr.prob(net, c)) return 0;
-  const uint64_t h2 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 2);
-  const bool glitch = u01(h2) < tp.glitch_p;
-  const uint64_t h3 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 3);
-  const int64_t lo0 = (c == 0) ? 1 : 0;  // tick 0 holds the initial value
-  if (!glitch) {
-    t[0] = base + lo0 + static_cast<int64_t>(u01(h3) * (tp.tpc - lo0));
-    return 1;
-  }
-  const uint64_t h4 = hash3(tp.seed, static_cast<uint64_t>(net), static_cast<uint64_t>(c), 4);
-  int64_t w = tp.w_lo + static_cast<int64_t>(u01(h4) * (tp.w_hi - tp.w_lo + 1));
-  if (2 * w >= tp.tpc - lo0) w = std::max<int64_t>(1, (tp.tpc - lo0 - 1) / 2);
-  const int64_t span = tp.tpc - lo0 - 2 * w;
-  const int64_t o = lo0 + static_cast<int64_t>(u01(h3) * span);
-  t[0] = base + o;
-  t[1] = base + o + w;
-  t[2] = base + o + 2 * w;
-  return 3;
+  return gtpb::syn::cycle_events(tr.rules, net, c, t);
 }
 
 }  // namespace
@@ -302,6 +276,7 @@ void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int6
       tr->phase[c] = ph;
     }
   }
+  tr->set_rules();
   return tr;
 }
 
@@ -324,6 +299,7 @@ void* synth_trace_create_phased(int32_t n_net, int32_t clock_net, int64_t n_cycl
   tr->act.resize(static_cast<size_t>(n_phase) * tp.n_unit);
   Rng ar(seed ^ 0xAC71u);
   for (double& a : tr->act) a = std::exp(act_sigma * ar.normal() - 0.5 * act_sigma * act_sigma);
+  tr->set_rules();
   return tr;
 }
 
@@ -635,8 +611,16 @@ int64_t synth_stream_next(void* h, int64_t* t_lo, int64_t* t_hi, int64_t* net_of
 // Initial net values (tick 0): a seeded coin per net; the clock starts at 0.
 void synth_trace_initial(void* h, uint8_t* init_value) {
   Trace* tr = static_cast<Trace*>(h);
-  for (int32_t n = 0; n < tr->tp.n_net; ++n)
-    init_value[n] = (n == tr->tp.clock_net) ? 0 : static_cast<uint8_t>(hash3(tr->tp.seed, n, 0xABCDEFull, 5) & 1);
+  for (int32_t n = 0; n < tr->tp.n_net; ++n) init_value[n] = gtpb::syn::initial_value(tr->rules, n);
+}
+
+// The trace's parameters and tables, for a generator elsewhere (the device
+// generator): fills *rules with host pointers into the trace, valid while the
+// trace lives; returns the number of phases (0 when the mode has none).
+int32_t synth_trace_rules(void* h, gtpb::syn::Rules* rules) {
+  Trace* tr = static_cast<Trace*>(h);
+  *rules = tr->rules;
+  return tr->tp.n_phase;
 }
 
 }  // extern "C"

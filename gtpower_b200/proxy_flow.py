@@ -27,6 +27,7 @@ import numpy as np
 from . import proxy as px
 from . import synth
 from .power import B200Power
+from .synth import DeviceWindow
 
 
 def _torch():
@@ -34,23 +35,19 @@ def _torch():
     return torch
 
 
-@dataclass
-class DeviceWindow:
-    """One window of events in device memory, in the gtp_events layout."""
-    c_lo: int
-    c_hi: int
-    t_lo: int
-    t_hi: int
-    n_event: int
-    net_off: object
-    time: object
-    packed: object
-    net_base: object
-
-    def push(self, eng: B200Power, t_lo: int | None = None, t_hi: int | None = None) -> None:
-        eng.push_device(self.n_event, self.net_off.data_ptr(), self.time.data_ptr(), self.packed.data_ptr(),
-                        self.net_base.data_ptr(), self.t_lo if t_lo is None else t_lo,
-                        self.t_hi if t_hi is None else t_hi)
+def generate_on_device(trace: synth.Trace, window_cycles: int, device: int = 0) -> list[DeviceWindow]:
+    """All windows of the trace, generated on the GPU (synth.DeviceStream)."""
+    torch = _torch()
+    st = synth.DeviceStream(trace, window_cycles, device)
+    out = []
+    while True:
+        w = st.next()
+        if w is None:
+            break
+        out.append(w)
+    torch.cuda.synchronize()
+    st.close()
+    return out
 
 
 def upload_trace(trace: synth.Trace, window_cycles: int, device: str = "cuda", threads: int = 0,

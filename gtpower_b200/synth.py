@@ -394,3 +394,115 @@ class Stream:
         packed = np.empty((n + 15) // 16, np.uint32)
         synth_lib().synth_pack_values(_p(values), n, _p(packed), self.threads)
         return Events(net_off, times[:n].copy(), packed, net_base=net_base, t_lo=t_lo, t_hi=t_hi)
+
+
+# ---------------------------------------------------------------------------
+# Device-side generation (synth_dev.cu): the same windows as Stream, written
+# straight into device memory.
+
+class _Rules(C.Structure):
+    """ctypes mirror of gtpb::syn::Rules (csrc/synth_rules.h)."""
+    _fields_ = [("mode", C.c_int32), ("clock_net", C.c_int32), ("n_net", C.c_int32), ("n_unit", C.c_int32),
+                ("n_cycle", C.c_int64), ("tpc", C.c_int64), ("seed", C.c_uint64), ("lo", C.c_double),
+                ("hi", C.c_double), ("glitch_p", C.c_double), ("w_lo", C.c_int64), ("w_hi", C.c_int64),
+                ("net_rate", C.c_void_p), ("burst", C.c_void_p), ("phase", C.c_void_p), ("act", C.c_void_p)]
+
+
+_dlib = None
+
+
+def synthdev_lib() -> C.CDLL:
+    global _dlib
+    if _dlib is None:
+        L = C.CDLL(build.build_synthdev())
+        L.synthdev_create.restype = C.c_void_p
+        L.synthdev_create.argtypes = [C.POINTER(_Rules), C.c_int32, C.c_int64, C.c_int32]
+        L.synthdev_destroy.argtypes = [C.c_void_p]
+        L.synthdev_count.restype = C.c_int64
+        L.synthdev_count.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.c_void_p]
+        L.synthdev_fill.restype = C.c_int32
+        L.synthdev_fill.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+        sl = synth_lib()
+        sl.synth_trace_rules.restype = C.c_int32
+        sl.synth_trace_rules.argtypes = [C.c_void_p, C.POINTER(_Rules)]
+        _dlib = L
+    return _dlib
+
+
+@dataclass
+class DeviceWindow:
+    """One window of events in device memory (torch tensors), in the
+    gtp_events layout: net_off int64 [n_net+1], time int64 [n_event],
+    packed int32 [ceil(n_event/16)] (2-bit values), net_base int64 [n_net]."""
+    c_lo: int
+    c_hi: int
+    t_lo: int
+    t_hi: int
+    n_event: int
+    net_off: object
+    time: object
+    packed: object
+    net_base: object
+
+    def push(self, eng, t_lo: int | None = None, t_hi: int | None = None) -> None:
+        """Evaluates this window (or the part [t_lo, t_hi) of it) on a
+        B200Power engine."""
+        eng.push_device(self.n_event, self.net_off.data_ptr(), self.time.data_ptr(), self.packed.data_ptr(),
+                        self.net_base.data_ptr(), self.t_lo if t_lo is None else t_lo,
+                        self.t_hi if t_hi is None else t_hi)
+
+
+class DeviceStream:
+    """Windows of a `Trace` generated on the GPU, identical to `Stream`'s."""
+
+    def __init__(self, trace: Trace, window_cycles: int, device: int = 0):
+        import torch
+        self.trace = trace
+        self.device = device
+        rules = _Rules()
+        L = synthdev_lib()
+        n_phase = synth_lib().synth_trace_rules(trace.h, C.byref(rules))
+        self.h = L.synthdev_create(C.byref(rules), n_phase, window_cycles, device)
+        if not self.h:
+            raise RuntimeError("synthdev_create failed")
+        self.n_net = trace.n_net
+        self.tpc = trace.tpc
+        self.n_cycle = trace.n_cycle
+        self._torch = torch
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            synthdev_lib().synthdev_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def next(self) -> DeviceWindow | None:
+        torch = self._torch
+        L = synthdev_lib()
+        dev = f"cuda:{self.device}"
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        net_off = torch.empty(self.n_net + 1, dtype=torch.int64, device=dev)
+        lo = C.c_int64()
+        hi = C.c_int64()
+        n = int(L.synthdev_count(self.h, net_off.data_ptr(), C.byref(lo), C.byref(hi), stream))
+        if n == -1:
+            return None
+        if n < 0:
+            raise RuntimeError("synthdev_count failed")
+        time = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+        packed = torch.empty(max((n + 15) // 16, 1), dtype=torch.int32, device=dev)
+        net_base = torch.empty(self.n_net, dtype=torch.int64, device=dev)
+        rc = L.synthdev_fill(self.h, net_off.data_ptr(), n, time.data_ptr(), packed.data_ptr(),
+                             net_base.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"synthdev_fill failed ({rc})")
+        c_lo, c_hi = lo.value, hi.value
+        t_hi = c_hi * self.tpc if c_hi < self.n_cycle else np.iinfo(np.int64).max
+        return DeviceWindow(c_lo, c_hi, c_lo * self.tpc, t_hi, n, net_off, time, packed, net_base)

@@ -18,7 +18,7 @@ def test_proxy_flow_phased_workload():
     d, info = synth.flat_design(synth.FlatSpec(n_cell=100000, n_cycle=12000, seed=31))
     spec = synth.TraceSpec(mode=3, lo=0.02, hi=0.12, n_phase=16, p_stay=0.99, n_unit=16, act_sigma=1.0)
     tr = synth.Trace(d, info, spec, seed=32)
-    wins = pf.upload_trace(tr, 1000)
+    wins = pf.generate_on_device(tr, 1000)
     assert sum(w.c_hi - w.c_lo for w in wins) == 12000
     rep = pf.run_flow(d, wins, info["tpc"], n_train=9000, n_block=16, k=2048, hidden=256, batch=512,
                       epochs=40, lr=1e-3, audit_frac=0.02, audit_run=10, seed=3,
