@@ -48,9 +48,14 @@ def parse():
     ap.add_argument("--cycles-per-tile", type=int, default=0)
     ap.add_argument("--gates-per-block", type=int, default=0)
     ap.add_argument("--threads-per-block", type=int, default=0)
-    ap.add_argument("--workload", default="flat", choices=["flat", "proxy"],
+    ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch"],
                     help="flat: the plain walk (default); proxy: the learned per-cycle power proxy "
-                         "against the plain walk on a phased-unit trace")
+                         "against the plain walk on a phased-unit trace; batch: 64 uneven traces x "
+                         "3 corners in persistent batched launches")
+    ap.add_argument("--batch-traces", type=int, default=64)
+    ap.add_argument("--batch-window", type=int, default=2048)
+    ap.add_argument("--batch-max-cells", type=int, default=500_000)
+    ap.add_argument("--batch-max-cycles", type=int, default=50_000)
     ap.add_argument("--proxy-cells", type=int, default=1_000_000)
     ap.add_argument("--proxy-cycles", type=int, default=100_000)
     ap.add_argument("--proxy-train", type=int, default=20_000)
@@ -202,6 +207,133 @@ def run_proxy(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """64 synthetic traces of uneven size (cells log-uniform in [1e4, 5e5],
+    cycles log-uniform in [1e3, 5e4], toggle U[0.05, 0.3], glitch p=0.05),
+    3 corners (leakage and internal tables x 0.8 / 1.0 / 1.3) folded from one
+    walk, in persistent batched launches window by window; block shape from
+    the autotuner. Windows are generated on the GPU before each timed push."""
+    import torch
+    from gtpower_b200 import B200Power, batch, synth
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(20261203 + 3)
+    n_tr = args.batch_traces
+    cells = np.exp(rng.uniform(np.log(1e4), np.log(args.batch_max_cells), n_tr)).astype(np.int64)
+    cycles = np.exp(rng.uniform(np.log(1e3), np.log(args.batch_max_cycles), n_tr)).astype(np.int64)
+    t0 = time.time()
+    designs, traces = [], []
+    for i in range(n_tr):
+        d, info = synth.flat_design(synth.FlatSpec(n_cell=int(cells[i]), n_cycle=int(cycles[i]),
+                                                   seed=20261203 + 3 + i))
+        designs.append(d)
+        traces.append(synth.Trace(d, info, synth.TraceSpec(), seed=20261203 + 3 + 1000 + i))
+    build_s = time.time() - t0
+    W = args.batch_window
+    log = lambda m: print("# " + m, file=sys.stderr, flush=True)
+    log(f"{n_tr} designs built in {build_s:.1f} s; cells {int(cells.sum())}, max cycles {int(cycles.max())}")
+    # autotune on the first windows of every 4th trace
+    sample = list(range(0, n_tr, 4))
+    sw = []
+    for i in sample:
+        st = synth.DeviceStream(traces[i], W)
+        sw.append(st.next())
+        st.close()
+    torch.cuda.synchronize()
+    best, table = batch.tune([designs[i] for i in sample], sw, log=log)
+    del sw
+    torch.cuda.empty_cache()
+    log(f"autotuner: {best}")
+    engines = [B200Power(d, **best.engine_kw()) for d in designs]
+    streams = [synth.DeviceStream(tr, W) for tr in traces]
+    bp = batch.BatchPower(engines)
+    s = torch.cuda.ExternalStream(bp.stream)
+    bufs = [None] * n_tr
+    total_ev = 0
+    walk_s = 0.0
+    gen_s = 0.0
+    waves = 0
+    seq_s = None
+    seq_ev = 0
+    batch_wave0_s = None
+    sampler = ClockSampler(0)
+    sampler.start()
+    while True:
+        g0 = time.time()
+        wins = [st.next(out=bufs[i]) if st is not None else None for i, st in enumerate(streams)]
+        for i, w in enumerate(wins):
+            if w is None and streams[i] is not None:
+                streams[i].close()
+                streams[i] = None
+            elif w is not None:
+                bufs[i] = w
+        torch.cuda.synchronize()
+        gen_s += time.time() - g0
+        if all(w is None for w in wins):
+            break
+        if waves == 0:  # the same windows one design at a time, for comparison
+            seq_eng = [B200Power(d, **best.engine_kw()) for d in designs]
+            batch.run_sequential(seq_eng, wins)          # warm-up
+            for e in seq_eng:
+                e.reset()
+            seq_s = batch.run_sequential(seq_eng, wins)
+            seq_ev = sum(w.n_event for w in wins if w is not None)
+            for e in seq_eng:
+                e.close()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        bp.push(wins)
+        b.record(s)
+        bp.sync()
+        dt = a.elapsed_time(b) / 1e3
+        if waves == 0:
+            batch_wave0_s = dt
+        walk_s += dt
+        total_ev += sum(w.n_event for w in wins if w is not None)
+        waves += 1
+    clocks = sampler.stop()
+    stats = bp.stats()
+    # corners folded from the one walk
+    f0 = time.time()
+    corner_totals = []
+    for e in engines:
+        r = e.fetch()
+        corner_totals.append([float(np.sum(batch.fold_corner(r, ls, is_).totals[[0, 1, 3]]))
+                              for ls, is_ in batch.CORNERS])
+    fold_s = time.time() - f0
+    bp.close()
+    peak, kind = measured_peak_hbm()
+    line = {
+        "metric": f"net events/s, batched persistent walk ({n_tr} uneven traces x 3 corners)",
+        "value": total_ev / walk_s, "unit": "events/s", "n_gpus": 1, "steps": waves, "warmup": 1,
+        "ms_per_step": walk_s * 1e3 / max(1, waves), "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{n_tr} flat synthetic traces, cells log-uniform [1e4, {args.batch_max_cells}], "
+                               f"cycles log-uniform [1e3, {args.batch_max_cycles}], toggle U[0.05,0.3], glitch 0.05; "
+                               f"corners x0.8/x1.0/x1.3 folded from one walk; windows of {W} cycles",
+                   "n_event_total": total_ev, "cells_total": int(cells.sum()),
+                   "cell_cycles_total": int((cells * cycles).sum()), "waves": waves,
+                   "autotuned_shape": best.__dict__,
+                   "autotune_ms": {f"{c.cycles_per_tile}/{c.threads_per_block}/{c.gates_per_block}": t * 1e3
+                                   for c, t in table},
+                   "design_build_s": build_s, "generation_s": gen_s},
+        "corner_events_per_s": 3 * total_ev / walk_s,
+        "cell_cycles_per_s": float((cells * cycles).sum()) / walk_s,
+        "first_wave": {"events": seq_ev,
+                       "one_design_at_a_time_events_per_s": seq_ev / seq_s if seq_s else None,
+                       "batched_events_per_s": seq_ev / batch_wave0_s if batch_wave0_s else None,
+                       "batched_speedup": (seq_s / batch_wave0_s) if (seq_s and batch_wave0_s) else None,
+                       "note": "batched time includes the host-side graph capture of its first push"},
+        "batch_stats": stats, "corner_fold_s": fold_s,
+        "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "traffic": None, "peak_source": kind, "kernel": "power_walk_batch_kernel"},
+        "clocks": clocks,
+    }
+    ab = 8.25 * total_ev / walk_s / 1e9
+    line["roofline"]["achieved"] = ab
+    line["roofline"]["frac"] = ab / peak
+    print(json.dumps(line), flush=True)
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -287,6 +419,10 @@ def main():
     if args.workload == "proxy":
         if rank == 0:
             run_proxy(args)
+        return
+    if args.workload == "batch":
+        if rank == 0:
+            run_batch(args)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -102,6 +102,10 @@ class gtp_proxy_config(C.Structure):
                 ("reserved32", C.c_int32), ("reserved", C.c_int64 * 4)]
 
 
+class gtp_batch_config(C.Structure):
+    _fields_ = [("use_graph", C.c_int32), ("blocks_per_sm", C.c_int32), ("reserved", C.c_int64 * 4)]
+
+
 # Every symbol the headers declare (include/gtpb200.h, include/gtpb200_proxy.h).
 EXPORTED = sorted([
     "gtp_config_default", "gtp_create", "gtp_destroy", "gtp_last_error", "gtp_n_period",
@@ -109,6 +113,8 @@ EXPORTED = sorted([
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
     "gtp_evaluate_noalloc", "gtp_pack_values",
     "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups",
+    "gtp_batch_config_default", "gtp_batch_create", "gtp_batch_destroy", "gtp_batch_last_error",
+    "gtp_batch_push_device", "gtp_batch_sync", "gtp_batch_get_stream", "gtp_batch_stats",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
     "gtp_proxy_get_stream", "gtp_proxy_set_stream", "gtp_proxy_n_param",
     "gtp_proxy_set_training_data", "gtp_proxy_get_norm", "gtp_proxy_train",

@@ -163,9 +163,12 @@ int64_t max_cycles_per_tile(int threads, int bin_sets) {
   return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (bin_sets * kNumCycAcc * 8 + 8)));
 }
 
-gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
-                      const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
-                      int64_t t_lo, int64_t t_hi) {
+// Validates one window and sets up its walk parameters *out (sorting the
+// walk order by work on `stream` when configured). The context's window
+// state advances only when the walk is enqueued (commit_window).
+gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t, const uint32_t* d_v,
+                          const int64_t* d_base, int64_t n_event, int64_t t_lo, int64_t t_hi,
+                          cudaStream_t stream, KParams* out, bool enqueue_sort = true) {
   if (t_hi <= t_lo) { c->err = "t_hi must exceed t_lo"; return GTP_EINVAL; }
   if (t_lo < 0) { c->err = "t_lo must be >= 0"; return GTP_EINVAL; }
   if (c->any_window && t_lo < c->last_t_hi) {
@@ -202,14 +205,41 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
-  const bool counts = c->cfg.collect_counts != 0;
   if (c->cfg.sort_by_work && c->d_order_work) {
-    cudaError_t e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in,
-                                       c->d_keys_out, c->d_order_work, c->d_sort_temp,
-                                       c->sort_temp_bytes, c->stream);
-    if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
+    if (enqueue_sort) {
+      cudaError_t e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in,
+                                         c->d_keys_out, c->d_order_work, c->d_sort_temp,
+                                         c->sort_temp_bytes, stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
+    }
     k.order = c->d_order_work;
   }
+  *out = k;
+  return GTP_OK;
+}
+
+// The work sort prepare_window(..., enqueue_sort = false) left to the caller.
+cudaError_t enqueue_window_sort(gtp_ctx* c, const KParams& k, cudaStream_t stream) {
+  if (!(c->cfg.sort_by_work && c->d_order_work)) return cudaSuccess;
+  const Packed& P = c->P;
+  return sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
+                            c->d_order_work, c->d_sort_temp, c->sort_temp_bytes, stream);
+}
+
+void commit_window(gtp_ctx* c, int64_t t_hi) {
+  c->any_window = true;
+  c->last_t_hi = t_hi;
+}
+
+gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
+                      const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
+                      int64_t t_lo, int64_t t_hi) {
+  KParams k;
+  gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, c->stream, &k);
+  if (st != GTP_OK) return st;
+  const Packed& P = c->P;
+  const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+  const bool counts = c->cfg.collect_counts != 0;
   static const int bucket_pins[3] = {4, 8, kMaxPins};
   for (int b = 0; b < 3; ++b) {
     k.order_begin = P.bucket_begin[b];
@@ -218,8 +248,7 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
     cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "power walk launch");
   }
-  c->any_window = true;
-  c->last_t_hi = t_hi;
+  commit_window(c, t_hi);
   return GTP_OK;
 }
 
@@ -595,6 +624,353 @@ gtp_status gtp_fetch_cycle_groups(gtp_ctx* c, float* cycle5_groups) {
                         cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "fetch cycle groups");
+  return GTP_OK;
+}
+
+}  // extern "C"
+
+// ---- batched evaluation: many contexts' windows in one persistent launch ----
+
+struct gtp_batch {
+  std::vector<gtp_ctx*> ctxs;
+  gtp_batch_config cfg{};
+  int device = 0;
+  int sm_count = 148;
+  int threads = 256;
+  bool counts = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // device and pinned staging copies of the walk parameters and work items
+  KParams* d_params = nullptr;
+  KParams* h_params = nullptr;
+  int params_cap = 0;
+  int4* d_items = nullptr;
+  int4* h_items = nullptr;
+  int64_t items_cap = 0;
+  int* d_meta = nullptr;  // per launch group g: [2g] item count, [2g+1] queue head
+  int* h_meta = nullptr;
+  cudaEvent_t ev = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<uint64_t> graph_key;
+  int64_t last_items = 0;
+  int last_launches = 0;
+  int graph_replays = 0;
+};
+
+namespace {
+
+constexpr int kBatchGroups = 6;  // pin bucket x drift
+
+void set_create_err(const std::string& m) {
+  std::lock_guard<std::mutex> g(g_err_mu);
+  g_create_err = m;
+}
+
+gtp_status batch_fail(gtp_batch* b, gtp_status st, const std::string& m) {
+  b->err = m;
+  return st;
+}
+
+void batch_release(gtp_batch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
+  if (b->d_params) cudaFree(b->d_params);
+  if (b->h_params) cudaFreeHost(b->h_params);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->h_items) cudaFreeHost(b->h_items);
+  if (b->d_meta) cudaFree(b->d_meta);
+  if (b->h_meta) cudaFreeHost(b->h_meta);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+struct BatchEntry {
+  int ctx;
+  int group;     // bucket * 2 + drift
+  int n_gblk;
+  int n_tiles;
+  int64_t ct;
+  int64_t cycles;  // cycles of the window
+  double density;  // events per net and cycle of the window
+  int32_t cells;   // cells of the bucket
+  int32_t gpb;
+};
+
+}  // namespace
+
+extern "C" {
+
+void gtp_batch_config_default(gtp_batch_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->use_graph = 1;
+  cfg->blocks_per_sm = 0;
+}
+
+gtp_status gtp_batch_create(gtp_ctx* const* ctxs, int32_t n_ctx, const gtp_batch_config* cfg, gtp_batch** out) {
+  if (!ctxs || !out || n_ctx < 1) return GTP_EINVAL;
+  *out = nullptr;
+  gtp_batch_config def;
+  gtp_batch_config_default(&def);
+  const gtp_batch_config& C = cfg ? *cfg : def;
+  int dev = -1, thr = -1, cnt = -1;
+  for (int i = 0; i < n_ctx; ++i) {
+    gtp_ctx* c = ctxs[i];
+    if (!c) return GTP_EINVAL;
+    const int t = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+    const int k = c->cfg.collect_counts ? 1 : 0;
+    if (i == 0) {
+      dev = c->device;
+      thr = t;
+      cnt = k;
+    } else if (c->device != dev || t != thr || k != cnt) {
+      set_create_err("gtp_batch_create: contexts must share the device, n_thread_per_block and collect_counts");
+      return GTP_EINVAL;
+    }
+  }
+  gtp_batch* b = new gtp_batch();
+  b->ctxs.assign(ctxs, ctxs + n_ctx);
+  b->cfg = C;
+  b->device = dev;
+  b->threads = thr;
+  b->counts = cnt != 0;
+  cudaError_t e = cudaSetDevice(dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_meta, sizeof(int) * 2 * kBatchGroups);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->h_meta, sizeof(int) * 2 * kBatchGroups);
+  if (e != cudaSuccess) {
+    set_create_err(std::string("gtp_batch_create: ") + cudaGetErrorString(e));
+    batch_release(b);
+    delete b;
+    return GTP_ECUDA;
+  }
+  *out = b;
+  return GTP_OK;
+}
+
+void gtp_batch_destroy(gtp_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_release(b);
+  delete b;
+}
+
+const char* gtp_batch_last_error(const gtp_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
+  if (!b || !d_ev) return GTP_EINVAL;
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, cudaGetErrorString(e));
+  // staging buffers of the previous push must be consumed
+  e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("sync: ") + cudaGetErrorString(e));
+  const int n = static_cast<int>(b->ctxs.size());
+  std::vector<KParams> params;
+  std::vector<BatchEntry> entries;
+  std::vector<int> active;
+  std::vector<KParams> kwin(n);
+  static const int bucket_pins[3] = {4, 8, kMaxPins};
+  for (int i = 0; i < n; ++i) {
+    const gtp_events& ev = d_ev[i];
+    if (ev.net_off == nullptr) continue;
+    gtp_ctx* c = b->ctxs[i];
+    if (ev.n_event < 0 || (ev.n_event > 0 && (!ev.time || !ev.value_packed)))
+      return batch_fail(b, GTP_EINVAL, "context " + std::to_string(i) + ": malformed events");
+    gtp_status st = prepare_window(c, ev.net_off, ev.time, ev.value_packed, ev.net_base, ev.n_event, ev.t_lo,
+                                   ev.t_hi, b->stream, &kwin[i], false);
+    if (st != GTP_OK) return batch_fail(b, st, "context " + std::to_string(i) + ": " + c->err);
+    active.push_back(i);
+    const KParams& k = kwin[i];
+    const Packed& P = c->P;
+    const int64_t cyc = static_cast<int64_t>(k.n_tiles) * k.cycles_per_tile;
+    const double dens = static_cast<double>(ev.n_event) / (std::max<double>(1.0, P.n_net) * std::max<int64_t>(1, cyc));
+    for (int bk = 0; bk < 3; ++bk) {
+      const int32_t lo = P.bucket_begin[bk], hi = P.bucket_begin[bk + 1];
+      if (hi <= lo) continue;
+      KParams kp = k;
+      kp.order_begin = lo;
+      kp.order_end = hi;
+      BatchEntry be;
+      be.ctx = i;
+      be.group = bk * 2 + (k.drift ? 1 : 0);
+      be.n_gblk = (hi - lo + k.gates_per_block - 1) / k.gates_per_block;
+      be.n_tiles = k.n_tiles;
+      be.ct = k.cycles_per_tile;
+      be.cycles = cyc;
+      be.density = dens;
+      be.cells = hi - lo;
+      be.gpb = k.gates_per_block;
+      params.push_back(kp);
+      entries.push_back(be);
+    }
+  }
+  if (active.empty()) return GTP_OK;
+  // work items per launch group, heaviest first
+  struct Item { double w; int4 v; };
+  std::vector<std::vector<Item>> groups(kBatchGroups);
+  size_t smem_g[kBatchGroups] = {0, 0, 0, 0, 0, 0};
+  for (size_t q = 0; q < entries.size(); ++q) {
+    const BatchEntry& be = entries[q];
+    const int bk = be.group / 2;
+    smem_g[be.group] = std::max(smem_g[be.group], walk_item_smem_bytes(params[q], bucket_pins[bk], b->counts, b->threads));
+    for (int g = 0; g < be.n_gblk; ++g) {
+      const int32_t cells = std::min<int32_t>(be.gpb, be.cells - g * be.gpb);
+      for (int t = 0; t < be.n_tiles; ++t) {
+        const int64_t cyc = std::min<int64_t>(be.ct, be.cycles - t * be.ct);
+        groups[be.group].push_back(Item{cells * static_cast<double>(cyc) * (be.density + 1e-3),
+                                        make_int4(static_cast<int>(q), g, t, 0)});
+      }
+    }
+  }
+  int64_t n_items = 0;
+  for (auto& g : groups) {
+    std::stable_sort(g.begin(), g.end(), [](const Item& x, const Item& y) { return x.w > y.w; });
+    n_items += static_cast<int64_t>(g.size());
+  }
+  if (n_items > INT32_MAX) return batch_fail(b, GTP_EOVERFLOW, "too many work items");
+  // staging (grown as needed; a capacity change invalidates the graph)
+  bool realloc = false;
+  if (static_cast<int>(params.size()) > b->params_cap) {
+    if (b->d_params) cudaFree(b->d_params);
+    if (b->h_params) cudaFreeHost(b->h_params);
+    b->params_cap = static_cast<int>(params.size()) * 2;
+    e = cudaMalloc(&b->d_params, sizeof(KParams) * b->params_cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_params, sizeof(KParams) * b->params_cap);
+    realloc = true;
+  }
+  if (e == cudaSuccess && n_items > b->items_cap) {
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->h_items) cudaFreeHost(b->h_items);
+    b->items_cap = n_items * 2;
+    e = cudaMalloc(&b->d_items, sizeof(int4) * b->items_cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_items, sizeof(int4) * b->items_cap);
+    realloc = true;
+  }
+  if (e != cudaSuccess) return batch_fail(b, GTP_ENOMEM, std::string("staging: ") + cudaGetErrorString(e));
+  std::memcpy(b->h_params, params.data(), sizeof(KParams) * params.size());
+  int64_t off = 0;
+  int64_t group_off[kBatchGroups];
+  for (int g = 0; g < kBatchGroups; ++g) {
+    group_off[g] = off;
+    for (const Item& it : groups[g]) b->h_items[off++] = it.v;
+    b->h_meta[2 * g] = static_cast<int>(groups[g].size());
+    b->h_meta[2 * g + 1] = 0;
+  }
+  // order against earlier work on the contexts' streams
+  for (int i : active) {
+    e = cudaEventRecord(b->ev, b->ctxs[i]->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev, 0);
+    if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("stream order: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemcpyAsync(b->d_params, b->h_params, sizeof(KParams) * params.size(), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_items, b->h_items, sizeof(int4) * std::max<int64_t>(1, n_items), cudaMemcpyHostToDevice,
+                        b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_meta, b->h_meta, sizeof(int) * 2 * kBatchGroups, cudaMemcpyHostToDevice, b->stream);
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
+  // the launch sequence: work sorts of every window, then one persistent
+  // walk per launch group. Its shape (contexts, buffers, grid, shared
+  // memory) keys the captured graph.
+  std::vector<uint64_t> key;
+  key.push_back(realloc ? 1u : 0u);
+  for (int i : active) {
+    key.push_back(static_cast<uint64_t>(i));
+    key.push_back(reinterpret_cast<uint64_t>(kwin[i].net_off));
+  }
+  int grid_g[kBatchGroups];
+  for (int g = 0; g < kBatchGroups; ++g) {
+    grid_g[g] = 0;
+    if (groups[g].empty()) continue;
+    const int bk = g / 2;
+    const int per_sm = b->cfg.blocks_per_sm > 0
+                           ? b->cfg.blocks_per_sm
+                           : walk_blocks_per_sm(bucket_pins[bk], b->counts, (g & 1) != 0, b->threads, smem_g[g]);
+    grid_g[g] = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(b->sm_count) * per_sm,
+                                                   static_cast<int64_t>(groups[g].size())));
+    key.push_back(static_cast<uint64_t>(g) << 56 | static_cast<uint64_t>(grid_g[g]) << 24 | smem_g[g]);
+  }
+  auto enqueue = [&]() -> cudaError_t {
+    cudaError_t r = cudaSuccess;
+    for (int i : active) {
+      r = enqueue_window_sort(b->ctxs[i], kwin[i], b->stream);
+      if (r != cudaSuccess) return r;
+    }
+    for (int g = 0; g < kBatchGroups; ++g) {
+      if (!grid_g[g]) continue;
+      r = launch_power_walk_batch(b->d_params, b->d_items + group_off[g], b->d_meta + 2 * g, b->d_meta + 2 * g + 1,
+                                  grid_g[g], bucket_pins[g / 2], b->counts, (g & 1) != 0, b->threads, smem_g[g],
+                                  b->stream);
+      if (r != cudaSuccess) return r;
+    }
+    return r;
+  };
+  int launches = 0;
+  for (int g = 0; g < kBatchGroups; ++g) launches += grid_g[g] ? 1 : 0;
+  if (b->cfg.use_graph) {
+    if (!b->gexec || key != b->graph_key) {
+      if (b->gexec) cudaGraphExecDestroy(b->gexec);
+      if (b->graph) cudaGraphDestroy(b->graph);
+      b->gexec = nullptr;
+      b->graph = nullptr;
+      e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t r = enqueue();
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(b->stream, &gr);
+        if (r != cudaSuccess) e = r;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->gexec, gr, 0);
+        if (e == cudaSuccess) {
+          b->graph = gr;
+          b->graph_key = key;
+        } else if (gr) {
+          cudaGraphDestroy(gr);
+        }
+      }
+    } else {
+      ++b->graph_replays;
+    }
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->gexec, b->stream);
+  } else {
+    e = enqueue();
+  }
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("batched walk: ") + cudaGetErrorString(e));
+  // later work on each context waits for the batch
+  e = cudaEventRecord(b->ev, b->stream);
+  for (int i : active) {
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->ctxs[i]->stream, b->ev, 0);
+    commit_window(b->ctxs[i], d_ev[i].t_hi);
+  }
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("stream order: ") + cudaGetErrorString(e));
+  b->last_items = n_items;
+  b->last_launches = launches;
+  return GTP_OK;
+}
+
+gtp_status gtp_batch_sync(gtp_batch* b) {
+  if (!b) return GTP_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("sync: ") + cudaGetErrorString(e));
+  for (size_t i = 0; i < b->ctxs.size(); ++i) {
+    gtp_status st = check_status(b->ctxs[i]);
+    if (st != GTP_OK) return batch_fail(b, st, "context " + std::to_string(i) + ": " + b->ctxs[i]->err);
+  }
+  return GTP_OK;
+}
+
+void* gtp_batch_get_stream(const gtp_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+gtp_status gtp_batch_stats(const gtp_batch* b, int64_t* items, int32_t* launches, int32_t* graph_replays) {
+  if (!b) return GTP_EINVAL;
+  if (items) *items = b->last_items;
+  if (launches) *launches = b->last_launches;
+  if (graph_replays) *graph_replays = b->graph_replays;
   return GTP_OK;
 }
 

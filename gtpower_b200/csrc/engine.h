@@ -180,6 +180,19 @@ constexpr int32_t kErrContext = 8;
 // Launches the walk over one bucket of cells. shared-memory bytes computed inside.
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
                               cudaStream_t stream);
+// Persistent walk over many designs' windows (one launch per pin bucket):
+// d_params holds one KParams per (design, bucket), d_items the work items
+// (x: params index, y: gate block, z: tile), *d_n_items their count and
+// *d_counter the queue head (zeroed before the launch). smem must cover the
+// largest item's shared memory.
+cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items, const int* d_n_items,
+                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, int threads,
+                                    size_t smem, cudaStream_t stream);
+// Dynamic shared memory of one walk block for these parameters.
+size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int threads);
+// Resident blocks per SM of the persistent walk at this shape.
+int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem);
+
 // bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group.
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets = 1);

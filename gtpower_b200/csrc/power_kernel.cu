@@ -222,9 +222,12 @@ __device__ float glitch_ratio(const KParams& p, int64_t e, int64_t lo, int64_t h
   return fminf(1.0f, __fmul_rn(r, r));
 }
 
+// One work item of the walk: the cells order[order_begin + gblk * gates_per_block ...]
+// of one pin bucket over cycle tile `tile` of the window, with the block's
+// dynamic shared memory `smem`. All threads of the block call it together.
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
-__global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const KParams p) {
-  extern __shared__ unsigned long long smem[];
+__device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile,
+                                           unsigned long long* smem) {
   const int64_t ct = p.cycles_per_tile;
   // per-cycle groups: two bin sets, for the block's first group and the next
   const int nset = p.cell_cgroup ? 2 : 1;
@@ -233,7 +236,6 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
   bins.sc = reinterpret_cast<uint32_t*>(smem + nset * kNumCycAcc * ct);
   bins.off = 0;
   bins.g = 0;
-  const int tile = blockIdx.y;
   bins.c_lo = p.cyc0 + static_cast<int64_t>(tile) * ct;
   bins.ct = ct;
   for (int64_t k = threadIdx.x; k < nset * kNumCycAcc * ct; k += blockDim.x) smem[k] = 0ull;
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
   const bool owns_initial = (tile == 0) && (p.t_lo == 0);
   const double P = p.period_d;
 
-  const int32_t g_begin = p.order_begin + blockIdx.x * p.gates_per_block;
+  const int32_t g_begin = p.order_begin + gblk * p.gates_per_block;
   const int32_t g_end = min(p.order_end, g_begin + p.gates_per_block);
   // cells are ordered by group within a bucket: the block's first cell has
   // its smallest group
@@ -716,6 +718,41 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
   }
 }
 
+// One window of one design: block (x, y) walks gate block x over tile y.
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+__global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
+  extern __shared__ unsigned long long smem[];
+  walk_block<MAXP, COUNTS, FAST, DRIFT>(p, blockIdx.x, blockIdx.y, smem);
+}
+
+// Persistent walk over the windows of many designs: each block takes work
+// items (x: index into params, one per design and pin bucket; y: gate block;
+// z: tile) from a queue in descending order of estimated work until it is
+// empty. *n_items and the queue head *counter live in device memory, so a
+// captured launch can be replayed with new items.
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+__global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
+    power_walk_batch_kernel(const KParams* __restrict__ params, const int4* __restrict__ items,
+                            const int* __restrict__ n_items, int* __restrict__ counter) {
+  extern __shared__ unsigned long long smem[];
+  __shared__ KParams sp;
+  __shared__ int s_item;
+  const int n = *n_items;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n) break;
+    const int4 w = items[it];
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(params + w.x);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sp);
+    for (int k = threadIdx.x; k < static_cast<int>(sizeof(KParams) / 8); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    walk_block<MAXP, COUNTS, FAST, DRIFT>(sp, w.y, w.z, smem);
+    __syncthreads();  // smem and s_item are reused by the next item
+  }
+}
+
 // ---- walk order by work ----
 
 __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
@@ -886,7 +923,64 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+cudaError_t launch_batch_t(const KParams* d_params, const int4* d_items, const int* d_n_items, int* d_counter,
+                           int grid, int threads, size_t smem, cudaStream_t stream) {
+  auto kern = power_walk_batch_kernel<MAXP, COUNTS, FAST, DRIFT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<grid, threads, smem, stream>>>(d_params, d_items, d_n_items, d_counter);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+static_assert(sizeof(KParams) % 8 == 0, "KParams is copied to shared memory in 8-byte words");
+
+cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items, const int* d_n_items,
+                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, int threads,
+                                    size_t smem, cudaStream_t stream) {
+  if (max_pins <= kFastPins) {
+    if (drift) return counts ? launch_batch_t<kFastPins, true, true, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                             : launch_batch_t<kFastPins, false, true, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+    return counts ? launch_batch_t<kFastPins, true, true, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                  : launch_batch_t<kFastPins, false, true, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+  }
+  if (max_pins <= 8) {
+    if (drift) return counts ? launch_batch_t<8, true, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                             : launch_batch_t<8, false, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+    return counts ? launch_batch_t<8, true, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                  : launch_batch_t<8, false, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+  }
+  if (drift) return counts ? launch_batch_t<kMaxPins, true, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                           : launch_batch_t<kMaxPins, false, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+  return counts ? launch_batch_t<kMaxPins, true, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
+                : launch_batch_t<kMaxPins, false, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+}
+
+int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem) {
+  int nb = 0;
+  cudaError_t e;
+  if (max_pins <= kFastPins)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kFastPins, false, true, true>, threads, smem);
+  else if (max_pins <= 8)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<8, false, false, true>, threads, smem);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kMaxPins, false, false, true>, threads, smem);
+  (void)counts;
+  (void)drift;
+  return e == cudaSuccess && nb > 0 ? nb : 1;
+}
+
+size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int threads) {
+  const bool fast = max_pins <= kFastPins;
+  size_t tabs = (fast && p.tabs_in_smem)
+                    ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16
+                    : 0;
+  if (fast && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
+  return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, (fast && WALK_USE_RING) ? kFastPins : 0, tabs,
+                               p.cell_cgroup ? 2 : 1);
+}
 
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets) {

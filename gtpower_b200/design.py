@@ -109,6 +109,25 @@ class CellLibrary:
         self.n_table = len(tables)
         self.n_cube = len(cubes)
 
+    def scaled(self, leak_scale: float = 1.0, int_scale: float = 1.0) -> "CellLibrary":
+        """The same library at another corner: every internal-power table's
+        scale factor times int_scale, every leakage value times leak_scale."""
+        import copy
+        L = copy.copy(self)
+        L.c_tables = (_abi.gtp_table * len(self.c_tables))()
+        for i, t in enumerate(self.c_tables):
+            L.c_tables[i] = _abi.gtp_table(t.order, t.axis1_var, t.axis2_var, t.n1, t.n2, t.axis1_off,
+                                           t.axis2_off, t.value_off, float(np.float32(t.scale * int_scale)), 0)
+        L.c_leak = (_abi.gtp_leakage_power * len(self.c_leak))()
+        for i, lp in enumerate(self.c_leak):
+            L.c_leak[i] = _abi.gtp_leakage_power(lp.when, float(np.float32(lp.power * leak_scale)), 0)
+        L.c_types = (_abi.gtp_cell_type * len(self.c_types))()
+        for i, t in enumerate(self.c_types):
+            L.c_types[i] = _abi.gtp_cell_type(t.n_pin, t.n_in, t.ipwr_off, t.n_ipwr, t.leak_off, t.n_leak,
+                                              float(np.float32(t.cell_leakage_power * leak_scale)),
+                                              t.has_cell_leakage_power)
+        return L
+
     def n_pin(self, t: int) -> int:
         return len(self.cells[t]["pins"])
 

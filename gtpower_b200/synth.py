@@ -483,12 +483,14 @@ class DeviceStream:
         except Exception:
             pass
 
-    def next(self) -> DeviceWindow | None:
+    def next(self, out: DeviceWindow | None = None) -> DeviceWindow | None:
+        """The next window, in new tensors or, when `out` is given and large
+        enough, in out's tensors (so that their addresses stay the same)."""
         torch = self._torch
         L = synthdev_lib()
         dev = f"cuda:{self.device}"
         stream = torch.cuda.current_stream(dev).cuda_stream
-        net_off = torch.empty(self.n_net + 1, dtype=torch.int64, device=dev)
+        net_off = out.net_off if out is not None else torch.empty(self.n_net + 1, dtype=torch.int64, device=dev)
         lo = C.c_int64()
         hi = C.c_int64()
         n = int(L.synthdev_count(self.h, net_off.data_ptr(), C.byref(lo), C.byref(hi), stream))
@@ -496,9 +498,12 @@ class DeviceStream:
             return None
         if n < 0:
             raise RuntimeError("synthdev_count failed")
-        time = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-        packed = torch.empty(max((n + 15) // 16, 1), dtype=torch.int32, device=dev)
-        net_base = torch.empty(self.n_net, dtype=torch.int64, device=dev)
+        if out is not None and out.time.numel() >= max(n, 1) and out.packed.numel() >= max((n + 15) // 16, 1):
+            time, packed, net_base = out.time, out.packed, out.net_base
+        else:
+            time = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+            packed = torch.empty(max((n + 15) // 16, 1), dtype=torch.int32, device=dev)
+            net_base = out.net_base if out is not None else torch.empty(self.n_net, dtype=torch.int64, device=dev)
         rc = L.synthdev_fill(self.h, net_off.data_ptr(), n, time.data_ptr(), packed.data_ptr(),
                              net_base.data_ptr(), stream)
         if rc != 0:

@@ -311,6 +311,39 @@ gtp_status  gtp_fetch_cycle_groups(gtp_ctx* ctx, float* cycle5_groups);
 gtp_status  gtp_evaluate_noalloc(gtp_ctx* ctx, const gtp_events* d_ev, float* d_cell5,
                                  float* d_cycle5, double* d_totals);
 
+/* Batched evaluation. No counterpart in the reference, which runs one
+ * design per CudaPower::power call (power/cuda/CudaPower.cu:1227-1337).
+ *
+ * A batch groups contexts (each with its own design, accumulators and
+ * windows) that share a device, n_thread_per_block and collect_counts.
+ * gtp_batch_push_device takes one device window per context (d_ev[i] as for
+ * gtp_push_events_device; d_ev[i].net_off == NULL skips context i) and walks
+ * all of them in one persistent launch per pin bucket: blocks take
+ * (context, gate block, cycle tile) work items from a device queue, heaviest
+ * first. With use_graph the launch sequence (the windows' work sorts and
+ * the persistent walks) is captured in a CUDA graph and replayed while the
+ * contexts and their window buffers stay the same. Results are read per
+ * context with gtp_fetch after gtp_batch_sync. */
+typedef struct gtp_batch_config {
+  int32_t use_graph;       /* 1 (default): replay captured launches */
+  int32_t blocks_per_sm;   /* persistent blocks per SM; 0 = occupancy */
+  int64_t reserved[4];
+} gtp_batch_config;
+typedef struct gtp_batch gtp_batch;
+
+void        gtp_batch_config_default(gtp_batch_config* cfg);
+gtp_status  gtp_batch_create(gtp_ctx* const* ctxs, int32_t n_ctx, const gtp_batch_config* cfg,
+                             gtp_batch** out);
+void        gtp_batch_destroy(gtp_batch* b);
+const char* gtp_batch_last_error(const gtp_batch* b);
+gtp_status  gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev);
+/* Waits for the batch and reports invalid events of any context. */
+gtp_status  gtp_batch_sync(gtp_batch* b);
+void*       gtp_batch_get_stream(const gtp_batch* b);
+/* Work items and persistent launches of the last push; graph replays so far. */
+gtp_status  gtp_batch_stats(const gtp_batch* b, int64_t* items, int32_t* launches,
+                            int32_t* graph_replays);
+
 /* Packs one value per byte (0..3) into the 2-bit layout of value_packed. */
 void        gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed);
 

@@ -34,7 +34,7 @@ def test_struct_layout_matches_c_compiler(tmp_path):
     import subprocess
     names = ["gtp_table", "gtp_when", "gtp_internal_power", "gtp_leakage_power",
              "gtp_cell_type", "gtp_design", "gtp_events", "gtp_config", "gtp_counts",
-             "gtp_proxy_config"]
+             "gtp_proxy_config", "gtp_batch_config"]
     src = tmp_path / "sz.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtpb200.h"',
              '#include "gtpb200_proxy.h"', "int main(void){"]
