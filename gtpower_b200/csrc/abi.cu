@@ -41,9 +41,18 @@ struct gtp_ctx {
   void* d_sort_temp = nullptr;
   size_t sort_temp_bytes = 0;
   // events (host-pushed windows)
-  int64_t ev_cap = 0, net_cap_set = 0;
-  int64_t *d_net_off = nullptr, *d_ev_t = nullptr, *d_net_base = nullptr;
-  uint32_t* d_ev_v = nullptr;
+  // events pushed from host memory: two device slots, filled on copy_stream
+  // while the walk of the other slot's window runs on `stream`
+  struct Slot {
+    int64_t cap = 0;
+    int64_t *d_net_off = nullptr, *d_ev_t = nullptr, *d_net_base = nullptr;
+    uint32_t* d_ev_v = nullptr;
+    cudaEvent_t free_ev = nullptr;  // the walk that read the slot is done
+    bool used = false;
+  } slot[2];
+  int next_slot = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copied_ev = nullptr;
   // accumulators and outputs
   double* d_cell_acc = nullptr;
   unsigned long long* d_cyc_acc = nullptr;
@@ -96,14 +105,20 @@ double fixed_point_scale(double bound) {
 void free_all(gtp_ctx* c) {
   void* ptrs[] = {c->d_cell_pin_off, c->d_cell_type, c->d_cell_inst, c->d_order, c->d_pin_net,
                   c->d_pin_slot, c->d_pin_flags, c->d_cell_group, c->d_pin_gden, c->d_pin_swe,
-                  c->d_leak_pool, c->d_inst, c->d_types, c->d_slots, c->d_cubes, c->d_net_off,
-                  c->d_ev_t, c->d_net_base, c->d_ev_v, c->d_cell_acc, c->d_cyc_acc,
+                  c->d_leak_pool, c->d_inst, c->d_types, c->d_slots, c->d_cubes,
+                  c->slot[0].d_net_off, c->slot[0].d_ev_t, c->slot[0].d_net_base, c->slot[0].d_ev_v,
+                  c->slot[1].d_net_off, c->slot[1].d_ev_t, c->slot[1].d_net_base, c->slot[1].d_ev_v,
+                  c->d_cell_acc, c->d_cyc_acc,
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g,
                   c->d_cycle5_g, c->d_leak_tmp_g};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (auto& sl : c->slot)
+    if (sl.free_ev) cudaEventDestroy(sl.free_ev);
+  if (c->copied_ev) cudaEventDestroy(c->copied_ev);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
 
@@ -422,40 +437,66 @@ gtp_status gtp_push_events(gtp_ctx* c, const gtp_events* ev) {
     return GTP_EOVERFLOW;
   }
   cudaError_t e = cudaSuccess;
-  if (ev->n_event > c->ev_cap || !c->d_net_off) {
-    // grow the event buffers (previous windows are complete once the stream drains)
-    e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return cuda_fail(c, e, "sync");
-    if (c->d_ev_t) cudaFree(c->d_ev_t);
-    if (c->d_ev_v) cudaFree(c->d_ev_v);
-    c->d_ev_t = nullptr;
-    c->d_ev_v = nullptr;
+  if (!c->copy_stream) {
+    e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->copied_ev, cudaEventDisableTiming);
+    for (auto& sl : c->slot)
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.free_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(c, e, "copy stream");
+  }
+  auto& sl = c->slot[c->next_slot];
+  // the walk that last read this slot must be done before it is overwritten
+  if (sl.used) {
+    e = cudaStreamWaitEvent(c->copy_stream, sl.free_ev, 0);
+    if (e != cudaSuccess) return cuda_fail(c, e, "slot order");
+  }
+  if (ev->n_event > sl.cap || !sl.d_net_off) {
+    if (sl.used) {
+      e = cudaEventSynchronize(sl.free_ev);
+      if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+    }
+    if (sl.d_ev_t) cudaFree(sl.d_ev_t);
+    if (sl.d_ev_v) cudaFree(sl.d_ev_v);
+    sl.d_ev_t = nullptr;
+    sl.d_ev_v = nullptr;
     const int64_t cap = std::max<int64_t>(ev->n_event, 16);
-    e = cudaMalloc(&c->d_ev_t, sizeof(int64_t) * cap);
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_ev_v, sizeof(uint32_t) * ((cap + 15) / 16));
+    e = cudaMalloc(&sl.d_ev_t, sizeof(int64_t) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&sl.d_ev_v, sizeof(uint32_t) * ((cap + 15) / 16));
     if (e != cudaSuccess) {
-      c->ev_cap = 0;
+      sl.cap = 0;
       c->err = std::string("event buffers: ") + cudaGetErrorString(e);
       return e == cudaErrorMemoryAllocation ? GTP_ENOMEM : GTP_ECUDA;
     }
-    c->ev_cap = cap;
-    if (!c->d_net_off) {
-      e = cudaMalloc(&c->d_net_off, sizeof(int64_t) * (nn + 1));
-      if (e == cudaSuccess) e = cudaMalloc(&c->d_net_base, sizeof(int64_t) * std::max(1, nn));
+    sl.cap = cap;
+    if (!sl.d_net_off) {
+      e = cudaMalloc(&sl.d_net_off, sizeof(int64_t) * (nn + 1));
+      if (e == cudaSuccess) e = cudaMalloc(&sl.d_net_base, sizeof(int64_t) * std::max(1, nn));
       if (e != cudaSuccess) return cuda_fail(c, e, "net buffers");
     }
   }
-  e = cudaMemcpyAsync(c->d_net_off, ev->net_off, sizeof(int64_t) * (nn + 1), cudaMemcpyHostToDevice, c->stream);
+  cudaStream_t cs = c->copy_stream;
+  e = cudaMemcpyAsync(sl.d_net_off, ev->net_off, sizeof(int64_t) * (nn + 1), cudaMemcpyHostToDevice, cs);
   if (e == cudaSuccess && ev->n_event > 0)
-    e = cudaMemcpyAsync(c->d_ev_t, ev->time, sizeof(int64_t) * ev->n_event, cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(sl.d_ev_t, ev->time, sizeof(int64_t) * ev->n_event, cudaMemcpyHostToDevice, cs);
   if (e == cudaSuccess && ev->n_event > 0)
-    e = cudaMemcpyAsync(c->d_ev_v, ev->value_packed, sizeof(uint32_t) * ((ev->n_event + 15) / 16),
-                        cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(sl.d_ev_v, ev->value_packed, sizeof(uint32_t) * ((ev->n_event + 15) / 16),
+                        cudaMemcpyHostToDevice, cs);
   if (e == cudaSuccess && ev->net_base)
-    e = cudaMemcpyAsync(c->d_net_base, ev->net_base, sizeof(int64_t) * nn, cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(sl.d_net_base, ev->net_base, sizeof(int64_t) * nn, cudaMemcpyHostToDevice, cs);
+  if (e == cudaSuccess) e = cudaEventRecord(c->copied_ev, cs);
+  // the caller's memory is no longer read once this returns; the walk of the
+  // previous window keeps running meanwhile
+  if (e == cudaSuccess) e = cudaEventSynchronize(c->copied_ev);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->copied_ev, 0);
   if (e != cudaSuccess) return cuda_fail(c, e, "event copy");
-  return run_window(c, c->d_net_off, c->d_ev_t, c->d_ev_v, ev->net_base ? c->d_net_base : nullptr,
-                    ev->n_event, ev->t_lo, ev->t_hi);
+  gtp_status st = run_window(c, sl.d_net_off, sl.d_ev_t, sl.d_ev_v, ev->net_base ? sl.d_net_base : nullptr,
+                             ev->n_event, ev->t_lo, ev->t_hi);
+  if (st != GTP_OK) return st;
+  e = cudaEventRecord(sl.free_ev, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "slot order");
+  sl.used = true;
+  c->next_slot ^= 1;
+  return GTP_OK;
 }
 
 gtp_status gtp_push_events_device(gtp_ctx* c, const gtp_events* ev) {

@@ -248,18 +248,16 @@ void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int6
     for (int32_t n = 0; n < n_net; ++n)
       tr->net_rate[n] = lo + (hi - lo) * u01(hash3(seed, n, 0xFFFFFFFFull, 9));
   } else if (mode == 1) {
-    // Zipf over a random rank permutation, scaled to the requested mean
+    // Zipf weights over a random rank permutation; per-cycle burst factors
+    // normalised to mean 1; the weights' scale k is chosen so that the
+    // toggle probability min(1, k * w[net] * burst[c]) averages rate_mean
+    // over nets and cycles (clipping included)
     std::vector<uint32_t> perm(n_net);
     for (int32_t n = 0; n < n_net; ++n) perm[n] = n;
     for (int32_t i = n_net - 1; i > 0; --i) std::swap(perm[i], perm[rng.below(i + 1)]);
     tr->net_rate.resize(n_net);
-    double sum = 0;
-    for (int32_t n = 0; n < n_net; ++n) {
+    for (int32_t n = 0; n < n_net; ++n)
       tr->net_rate[n] = 1.0 / std::pow(static_cast<double>(perm[n]) + 1.0, zipf_alpha);
-      sum += tr->net_rate[n];
-    }
-    const double k = rate_mean * n_net / sum;
-    for (int32_t n = 0; n < n_net; ++n) tr->net_rate[n] = std::min(1.0, tr->net_rate[n] * k);
     tr->burst.resize(n_cycle);
     double bs = 0;
     for (int64_t c = 0; c < n_cycle; ++c) {
@@ -268,6 +266,31 @@ void* synth_trace_create(int32_t n_net, int32_t clock_net, int64_t n_cycle, int6
     }
     const double m = bs / std::max<int64_t>(1, n_cycle);
     for (int64_t c = 0; c < n_cycle; ++c) tr->burst[c] /= m;
+    // mean rate for scale k over the sorted weights and (a sample of) the bursts
+    std::vector<double> w(tr->net_rate);
+    std::sort(w.begin(), w.end());
+    std::vector<double> pre(w.size() + 1, 0.0);
+    for (size_t i = 0; i < w.size(); ++i) pre[i + 1] = pre[i] + w[i];
+    const int64_t stride = std::max<int64_t>(1, n_cycle / 4096);
+    auto mean_rate = [&](double k) {
+      double acc = 0;
+      int64_t cnt = 0;
+      for (int64_t c = 0; c < n_cycle; c += stride, ++cnt) {
+        const double kb = k * tr->burst[c];
+        const size_t j = static_cast<size_t>(std::upper_bound(w.begin(), w.end(), 1.0 / kb) - w.begin());
+        acc += kb * pre[j] + static_cast<double>(w.size() - j);
+      }
+      return acc / (static_cast<double>(w.size()) * std::max<int64_t>(1, cnt));
+    };
+    double k_lo = 0.0, k_hi = rate_mean * n_net / std::max(pre.back(), 1e-300);
+    const double target = std::min(rate_mean, 1.0);
+    for (int it = 0; it < 200 && mean_rate(k_hi) < target && target < 1.0; ++it) k_hi *= 2.0;
+    for (int it = 0; it < 100; ++it) {
+      const double mid = 0.5 * (k_lo + k_hi);
+      if (mean_rate(mid) < target) k_lo = mid;
+      else k_hi = mid;
+    }
+    for (int32_t n = 0; n < n_net; ++n) tr->net_rate[n] *= k_hi;
   } else {
     tr->phase.resize(n_cycle);
     uint8_t ph = static_cast<uint8_t>(rng.below(n_phase));

@@ -124,3 +124,31 @@ def test_cycle_groups_match_oracle_on_cell_subsets(n_group, layout, gpb, sort_by
         err = np.abs(G[g].T.astype(np.float64) - ref)
         assert (err <= tol).all(), (g, np.argwhere(err > tol)[:5].tolist())
     close("sum of groups", G.sum(0).T, full.cycle5.T)
+
+
+def test_host_buffers_may_be_reused_when_push_returns():
+    """gtp_push_events reads caller memory only until it returns (its copies
+    overlap the previous window's walk): scribbling over each window's host
+    arrays right after the push leaves the results unchanged."""
+    import torch
+    from gtpower_b200 import B200Power, synth
+    from gtpower_b200.design import Events
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=2500, n_cycle=120, seed=17))
+    spec = synth.TraceSpec(mode=1, glitch_p=0.1)
+    full = synth.Trace(d, info, spec, seed=18).full()
+    st = synth.Stream(synth.Trace(d, info, spec, seed=18), 13)
+    with B200Power(d, collect_counts=True, cycles_per_tile=5) as eng:
+        while True:
+            w = st.next(2_000_000)
+            if w is None:
+                break
+            pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                   for a in (w.net_off, w.time, w.packed.view(np.int32), w.net_base)]
+            ev = Events(pin[0].numpy(), pin[1].numpy(), pin[2].numpy().view(np.uint32), net_base=pin[3].numpy(),
+                        t_lo=w.t_lo, t_hi=w.t_hi)
+            eng.read_power_activities(ev)
+            for p in pin[1:]:
+                p.fill_(-1)
+        eng.sync()
+        res = eng.fetch(counts=True)
+    compare(res, oracle(d, full))
