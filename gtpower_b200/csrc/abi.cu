@@ -69,6 +69,9 @@ struct gtp_ctx {
   // per-cycle waveforms by cell group (gtp_set_cycle_groups)
   int32_t n_cgroup = 0;
   int32_t* d_cgroup = nullptr;
+  // per-window table of each (tile, net)'s first event
+  int32_t* d_tile_first = nullptr;
+  int64_t tile_first_cap = 0;
   unsigned long long* d_cyc_acc_g = nullptr;
   float* d_cycle5_g = nullptr;
   unsigned long long* d_leak_tmp_g = nullptr;
@@ -111,7 +114,7 @@ void free_all(gtp_ctx* c) {
                   c->d_cell_acc, c->d_cyc_acc,
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
-                  c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g,
+                  c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first,
                   c->d_cycle5_g, c->d_leak_tmp_g};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -151,6 +154,10 @@ KParams make_params(gtp_ctx* c) {
   k.n_net = P.n_net;
   k.tpc = P.tpc;
   k.inv_tpc = 1.0 / static_cast<double>(P.tpc);
+  k.tpc_magic = P.tpc >= 2 && P.tpc < (int64_t(1) << 31)
+                    ? static_cast<uint32_t>(((uint64_t(1) << 32) + static_cast<uint64_t>(P.tpc) - 1) /
+                                            static_cast<uint64_t>(P.tpc))
+                    : 0u;
   k.ts = P.ts;
   k.period_d = P.period_d;
   k.inv_period_d = 1.0 / P.period_d;
@@ -183,7 +190,7 @@ int64_t max_cycles_per_tile(int threads, int bin_sets) {
 // state advances only when the walk is enqueued (commit_window).
 gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t, const uint32_t* d_v,
                           const int64_t* d_base, int64_t n_event, int64_t t_lo, int64_t t_hi,
-                          cudaStream_t stream, KParams* out, bool enqueue_sort = true) {
+                          cudaStream_t stream, KParams* out, bool enqueue_prep = true) {
   if (t_hi <= t_lo) { c->err = "t_hi must exceed t_lo"; return GTP_EINVAL; }
   if (t_lo < 0) { c->err = "t_lo must be >= 0"; return GTP_EINVAL; }
   if (c->any_window && t_lo < c->last_t_hi) {
@@ -220,21 +227,44 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
-  if (c->cfg.sort_by_work && c->d_order_work) {
-    if (enqueue_sort) {
-      cudaError_t e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in,
-                                         c->d_keys_out, c->d_order_work, c->d_sort_temp,
-                                         c->sort_temp_bytes, stream);
+  // the (tile, net) first-event table, when it stays within kTileFirstMaxEntries
+  const int64_t entries = static_cast<int64_t>(k.n_tiles) * P.n_net;
+  if (entries > 0 && entries <= kTileFirstMaxEntries) {
+    if (entries > c->tile_first_cap) {
+      cudaError_t e = cudaStreamSynchronize(stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+      if (c->d_tile_first) cudaFree(c->d_tile_first);
+      c->d_tile_first = nullptr;
+      c->tile_first_cap = 0;
+      const int64_t cap = std::min<int64_t>(kTileFirstMaxEntries, entries * 2);
+      e = cudaMalloc(&c->d_tile_first, sizeof(int32_t) * cap);
+      if (e == cudaSuccess) c->tile_first_cap = cap;
+    }
+    if (c->d_tile_first) k.tile_first = c->d_tile_first;
+  }
+  if (c->cfg.sort_by_work && c->d_order_work) k.order = c->d_order_work;
+  if (enqueue_prep) {
+    cudaError_t e = cudaSuccess;
+    if (k.tile_first) e = launch_tile_first(k, nullptr, c->d_tile_first, stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "tile index");
+    if (c->cfg.sort_by_work && c->d_order_work) {
+      e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
+                             c->d_order_work, c->d_sort_temp, c->sort_temp_bytes, stream);
       if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
     }
-    k.order = c->d_order_work;
   }
   *out = k;
   return GTP_OK;
 }
 
-// The work sort prepare_window(..., enqueue_sort = false) left to the caller.
-cudaError_t enqueue_window_sort(gtp_ctx* c, const KParams& k, cudaStream_t stream) {
+// The per-window preparation prepare_window(..., enqueue_prep = false) left
+// to the caller; d_k: the window's parameters in device memory.
+cudaError_t enqueue_window_prep(gtp_ctx* c, const KParams& k, const KParams* d_k, cudaStream_t stream) {
+  if (k.tile_first) {
+    cudaError_t e = launch_tile_first(k, d_k, c->d_tile_first, stream);
+    if (e != cudaSuccess) return e;
+  }
   if (!(c->cfg.sort_by_work && c->d_order_work)) return cudaSuccess;
   const Packed& P = c->P;
   return sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
@@ -816,6 +846,7 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
   std::vector<BatchEntry> entries;
   std::vector<int> active;
   std::vector<KParams> kwin(n);
+  std::vector<int> first_entry(n, -1);
   static const int bucket_pins[3] = {4, 8, kMaxPins};
   for (int i = 0; i < n; ++i) {
     const gtp_events& ev = d_ev[i];
@@ -834,6 +865,7 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     for (int bk = 0; bk < 3; ++bk) {
       const int32_t lo = P.bucket_begin[bk], hi = P.bucket_begin[bk + 1];
       if (hi <= lo) continue;
+      if (first_entry[i] < 0) first_entry[i] = static_cast<int>(params.size());
       KParams kp = k;
       kp.order_begin = lo;
       kp.order_end = hi;
@@ -921,9 +953,12 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
   // memory) keys the captured graph.
   std::vector<uint64_t> key;
   key.push_back(realloc ? 1u : 0u);
+  key.push_back(reinterpret_cast<uint64_t>(b->d_params));
   for (int i : active) {
     key.push_back(static_cast<uint64_t>(i));
     key.push_back(reinterpret_cast<uint64_t>(kwin[i].net_off));
+    key.push_back(reinterpret_cast<uint64_t>(kwin[i].tile_first));
+    key.push_back(static_cast<uint64_t>(first_entry[i]));
   }
   int grid_g[kBatchGroups];
   for (int g = 0; g < kBatchGroups; ++g) {
@@ -940,7 +975,8 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
   auto enqueue = [&]() -> cudaError_t {
     cudaError_t r = cudaSuccess;
     for (int i : active) {
-      r = enqueue_window_sort(b->ctxs[i], kwin[i], b->stream);
+      const KParams* dk = first_entry[i] >= 0 ? b->d_params + first_entry[i] : nullptr;
+      r = enqueue_window_prep(b->ctxs[i], kwin[i], dk, b->stream);
       if (r != cudaSuccess) return r;
     }
     for (int g = 0; g < kBatchGroups; ++g) {

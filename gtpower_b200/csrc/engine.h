@@ -134,12 +134,15 @@ struct KParams {
   const int64_t* ev_t;
   const uint32_t* ev_v;
   const int64_t* net_base;   // may be null
+  const int32_t* tile_first; // [n_tiles][n_net] first event at or after each tile's start,
+                             // relative to net_off; null: the walk bisects
   int64_t n_event;
   int64_t t_lo, t_hi;
   int32_t n_net;
   // time base
   int64_t tpc;
   double inv_tpc;
+  uint32_t tpc_magic;        // ceil(2^32 / tpc) for tpc >= 2 (32-bit division by tpc), 0 for tpc == 1
   double ts;
   double period_d;
   double inv_period_d;
@@ -169,6 +172,9 @@ struct KParams {
 };
 
 // status bits set by the kernel
+// largest (tile, net) first-event table built per window (int32 entries)
+constexpr int64_t kTileFirstMaxEntries = int64_t(1) << 27;
+
 // largest number of per-cycle cell groups (sort keys hold the group in 18 bits)
 constexpr int32_t kMaxCycleGroups = 65536;
 
@@ -196,6 +202,10 @@ int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_
 // bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group.
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets = 1);
+
+// Builds p.tile_first's table (into `out`, n_tiles * n_net entries) for the
+// window p describes; with d_p set the kernel reads the window from there.
+cudaError_t launch_tile_first(const KParams& p, const KParams* d_p, int32_t* out, cudaStream_t stream);
 
 // Walk order for one window: cells stay grouped by pin bucket and, within a
 // bucket, by cell group when groups are set, and are sorted by the number of

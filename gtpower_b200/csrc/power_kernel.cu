@@ -64,6 +64,15 @@ __device__ __forceinline__ int64_t div_floor_pos(int64_t t, int64_t d, double in
   return q;
 }
 
+// floor(n / d) for n < 2^31, d < 2^31 with magic = ceil(2^32 / d) (d >= 2):
+// umulhi(n, magic) is floor(n / d) or one more.
+__device__ __forceinline__ uint32_t udiv32(uint32_t n, uint32_t d, uint32_t magic) {
+  if (magic == 0u) return n;  // d == 1
+  uint32_t q = __umulhi(n, magic);
+  if (q * d > n) --q;
+  return q;
+}
+
 __device__ __forceinline__ int ev_value(const uint32_t* __restrict__ v, int64_t i) {
   return (__ldg(v + (i >> 4)) >> (2 * (i & 15))) & 3;
 }
@@ -265,6 +274,9 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 
   // tile window in ticks: [T0, T0 + span)
   const int64_t T0 = max(p.t_lo, bins.c_lo * p.tpc);
+  // T0's offset within cycle c_lo: event cycles follow from 32-bit offsets
+  const uint32_t off0 = static_cast<uint32_t>(T0 - bins.c_lo * p.tpc);
+  const uint32_t tpc32 = static_cast<uint32_t>(p.tpc);
   const bool last_tile = (tile == p.n_tiles - 1);
   const int64_t T1 = last_tile ? min(p.t_hi, p.tmax + 1) : min(p.t_hi, (bins.c_lo + ct) * p.tpc);
   const uint32_t span = static_cast<uint32_t>(T1 > T0 ? T1 - T0 : 0);
@@ -383,11 +395,16 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
           } else if (e > a) {
             has_wave |= 1u << i;
             const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
-            // lower_bound(T0) in [a, e)
+            // lower_bound(T0) in [a, e): from the window's per-(tile, net)
+            // index when it was built, else by bisection
             int64_t l = a, r = e;
-            while (l < r) {
-              const int64_t m = l + ((r - l) >> 1);
-              if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
+            if (p.tile_first) {
+              l = a + __ldg(p.tile_first + static_cast<int64_t>(tile) * p.n_net + net);
+            } else {
+              while (l < r) {
+                const int64_t m = l + ((r - l) >> 1);
+                if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
+              }
             }
             // the waveform's first event at tick 0 is the initial condition
             if (l < e && l == a && base == 0 && ev_time(p.ev_t, l) == 0) ++l;
@@ -461,9 +478,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         if (i < n_pin) cur = min(cur, nt[i]);
       if (cur >= span) break;
       const int64_t cur_abs = T0 + cur;
-      const int64_t cyc = div_floor_pos(cur_abs, p.tpc, p.inv_tpc);
-      const int32_t cs_rel = static_cast<int32_t>(cyc * p.tpc - T0);   // cycle start - T0
-      const int32_t ce_rel = cs_rel + static_cast<int32_t>(p.tpc);
+      const uint32_t cq = udiv32(cur + off0, tpc32, p.tpc_magic);     // cycles after c_lo
+      const int64_t cyc = bins.c_lo + cq;
+      const int32_t cs_rel = static_cast<int32_t>(cq * tpc32) - static_cast<int32_t>(off0);  // cycle start - T0
+      const int32_t ce_rel = cs_rel + static_cast<int32_t>(tpc32);
 
       // advance every pin with an event at cur
       const uint32_t old_state = state;
@@ -753,6 +771,35 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
   }
 }
 
+// ---- first event of every (tile, net) ----
+
+// out[tile * n_net + net] = lower_bound(T0(tile)) - net_off[net] over the
+// net's events, T0(tile) = max(t_lo, (cyc0 + tile * cycles_per_tile) * tpc).
+// Parameters come from *pd when it is set (device memory, so that a captured
+// launch sees each window's values), else from pv.
+__global__ void tile_first_kernel(const KParams pv, const KParams* __restrict__ pd, int32_t* __restrict__ out) {
+  const KParams& p = pd ? *pd : pv;
+  const int64_t nn = p.n_net;
+  const int64_t total = static_cast<int64_t>(p.n_tiles) * nn;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t tile = i / nn;
+    const int32_t net = static_cast<int32_t>(i - tile * nn);
+    const int64_t T0 = max(p.t_lo, (p.cyc0 + tile * p.cycles_per_tile) * p.tpc);
+    const int64_t a = p.net_off[net], e = p.net_off[net + 1];
+    int64_t l = a, r = e;
+    if (a < 0 || e < a || e > p.n_event) {  // reported by the walk
+      out[i] = 0;
+      continue;
+    }
+    while (l < r) {
+      const int64_t m = l + ((r - l) >> 1);
+      if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
+    }
+    out[i] = static_cast<int32_t>(l - a);
+  }
+}
+
 // ---- walk order by work ----
 
 __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
@@ -778,6 +825,14 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
 }
 
 }  // namespace
+
+cudaError_t launch_tile_first(const KParams& p, const KParams* d_p, int32_t* out, cudaStream_t stream) {
+  const int64_t total = static_cast<int64_t>(p.n_tiles) * p.n_net;
+  if (total <= 0) return cudaSuccess;
+  const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 32));
+  tile_first_kernel<<<blocks, 256, 0, stream>>>(p, d_p, out);
+  return cudaGetLastError();
+}
 
 size_t work_sort_temp_bytes(int32_t n_cell) {
   size_t bytes = 0;
