@@ -72,6 +72,9 @@ struct gtp_ctx {
   // per-window table of each (tile, net)'s first event
   int32_t* d_tile_first = nullptr;
   int64_t tile_first_cap = 0;
+  // per-window glitch pulse width of each listed event
+  float* d_glitch_pw = nullptr;
+  int64_t glitch_pw_cap = 0;
   unsigned long long* d_cyc_acc_g = nullptr;
   float* d_cycle5_g = nullptr;
   unsigned long long* d_leak_tmp_g = nullptr;
@@ -114,7 +117,7 @@ void free_all(gtp_ctx* c) {
                   c->d_cell_acc, c->d_cyc_acc,
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
-                  c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first,
+                  c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
                   c->d_cycle5_g, c->d_leak_tmp_g};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -212,7 +215,7 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   const int64_t cyc_end = last_tick / P.tpc + 1;
   const int64_t n_cyc = std::max<int64_t>(1, cyc_end - k.cyc0);
   int64_t ct = c->cfg.cycles_per_tile;
-  if (ct <= 0) ct = 512;
+  if (ct <= 0) ct = c->n_cgroup > 0 ? 512 : 1024;  // per-group bins double the tile's shared memory
   ct = std::min<int64_t>(ct, n_cyc);
   const int threads_ = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   // bins + event buffers + tables within 227 KB of shared memory; tile span
@@ -226,7 +229,7 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   k.cycles_per_tile = ct;
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
-  k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads * 4;
+  k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads;
   // the (tile, net) first-event table, when it stays within kTileFirstMaxEntries
   const int64_t entries = static_cast<int64_t>(k.n_tiles) * P.n_net;
   if (entries > 0 && entries <= kTileFirstMaxEntries) {
@@ -243,10 +246,26 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     }
     if (c->d_tile_first) k.tile_first = c->d_tile_first;
   }
+  // the glitch widths of the window's events, within kGlitchPwMaxEvents
+  if (n_event > 0 && n_event <= kGlitchPwMaxEvents) {
+    if (n_event > c->glitch_pw_cap) {
+      cudaError_t e = cudaStreamSynchronize(stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+      if (c->d_glitch_pw) cudaFree(c->d_glitch_pw);
+      c->d_glitch_pw = nullptr;
+      c->glitch_pw_cap = 0;
+      const int64_t cap = std::min<int64_t>(kGlitchPwMaxEvents, n_event + n_event / 4 + 1024);
+      e = cudaMalloc(&c->d_glitch_pw, sizeof(float) * cap);
+      if (e == cudaSuccess) c->glitch_pw_cap = cap;
+    }
+    if (c->d_glitch_pw) k.glitch_pw = c->d_glitch_pw;
+  }
   if (c->cfg.sort_by_work && c->d_order_work) k.order = c->d_order_work;
   if (enqueue_prep) {
     cudaError_t e = cudaSuccess;
     if (k.tile_first) e = launch_tile_first(k, nullptr, c->d_tile_first, stream);
+    if (e == cudaSuccess && k.glitch_pw) e = launch_glitch_pw(k, nullptr, c->d_glitch_pw, stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tile index");
     if (c->cfg.sort_by_work && c->d_order_work) {
       e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
@@ -263,6 +282,10 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
 cudaError_t enqueue_window_prep(gtp_ctx* c, const KParams& k, const KParams* d_k, cudaStream_t stream) {
   if (k.tile_first) {
     cudaError_t e = launch_tile_first(k, d_k, c->d_tile_first, stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (k.glitch_pw) {
+    cudaError_t e = launch_glitch_pw(k, d_k, c->d_glitch_pw, stream);
     if (e != cudaSuccess) return e;
   }
   if (!(c->cfg.sort_by_work && c->d_order_work)) return cudaSuccess;
@@ -958,6 +981,7 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     key.push_back(static_cast<uint64_t>(i));
     key.push_back(reinterpret_cast<uint64_t>(kwin[i].net_off));
     key.push_back(reinterpret_cast<uint64_t>(kwin[i].tile_first));
+    key.push_back(reinterpret_cast<uint64_t>(kwin[i].glitch_pw));
     key.push_back(static_cast<uint64_t>(first_entry[i]));
   }
   int grid_g[kBatchGroups];

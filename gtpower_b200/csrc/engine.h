@@ -136,6 +136,8 @@ struct KParams {
   const int64_t* net_base;   // may be null
   const int32_t* tile_first; // [n_tiles][n_net] first event at or after each tile's start,
                              // relative to net_off; null: the walk bisects
+  const float* glitch_pw;    // [n_event] glitch pulse width (s) of each listed event, -1 when
+                             // not a glitch event; null: the walk classifies
   int64_t n_event;
   int64_t t_lo, t_hi;
   int32_t n_net;
@@ -172,6 +174,9 @@ struct KParams {
 };
 
 // status bits set by the kernel
+// largest window whose glitch widths are precomputed (float per event)
+constexpr int64_t kGlitchPwMaxEvents = int64_t(1) << 30;
+
 // largest (tile, net) first-event table built per window (int32 entries)
 constexpr int64_t kTileFirstMaxEntries = int64_t(1) << 27;
 
@@ -202,6 +207,10 @@ int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_
 // bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group.
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets = 1);
+
+// Fills p.glitch_pw's array (`out`, n_event entries) for the window p
+// describes; with d_p set the kernel reads the window from there.
+cudaError_t launch_glitch_pw(const KParams& p, const KParams* d_p, float* out, cudaStream_t stream);
 
 // Builds p.tile_first's table (into `out`, n_tiles * n_net entries) for the
 // window p describes; with d_p set the kernel reads the window from there.

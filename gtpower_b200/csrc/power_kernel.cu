@@ -184,11 +184,12 @@ __device__ __forceinline__ Group period_group(const int64_t* __restrict__ t, int
   return g;
 }
 
-// Glitch scaling ratio of event e on a net (getGlitchScalingRatioClockCycleBasedH
-// and getTimeBasedGlitchScalingRatioH, TimeBasedPower.cc:303-339,
-// PowerUtils.cc:285-294); -1 when the event is not a glitch event.
-__device__ float glitch_ratio(const KParams& p, int64_t e, int64_t lo, int64_t hi, int64_t g0,
-                              int64_t cur, int64_t cyc_start, float den) {
+// Pulse width of event e on a net as float seconds, -1 when the event is not
+// a glitch event (getGlitchScalingRatioClockCycleBasedH,
+// TimeBasedPower.cc:303-339: flags from whole-waveform period groups, width
+// to the previous or next event only when that neighbour is flagged).
+__device__ float glitch_pw(const KParams& p, int64_t e, int64_t lo, int64_t hi, int64_t g0,
+                           int64_t cur, int64_t cyc_start) {
   if (e == g0) return -1.0f;
   const Group gr = period_group(p.ev_t, e, lo, hi, g0, cyc_start, cyc_start + p.tpc);
   const int64_t k = gr.last - gr.first + 1;
@@ -224,11 +225,24 @@ __device__ float glitch_ratio(const KParams& p, int64_t e, int64_t lo, int64_t h
     if (nflag) w = max(w, tn - cur);
   }
   if (w < 0) return -1.0f;
+  return __double2float_rn(__dmul_rn(static_cast<double>(w), p.ts));
+}
+
+// Glitch scaling ratio for pulse width pw (s) on a pin whose rise and fall
+// slews sum to den (getTimeBasedGlitchScalingRatioH, PowerUtils.cc:285-294);
+// -1 when pw < 0 (not a glitch event).
+__device__ __forceinline__ float glitch_ratio_of(float pw, float den) {
+  if (pw < 0.0f) return -1.0f;
   if (den == 0.0f) return 1.0f;
-  const float pw = __double2float_rn(__dmul_rn(static_cast<double>(w), p.ts));
   const float r = __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(pw), 2.0),
                                               static_cast<double>(den)));
   return fminf(1.0f, __fmul_rn(r, r));
+}
+
+// glitch_pw and glitch_ratio_of in one step.
+__device__ __forceinline__ float glitch_ratio(const KParams& p, int64_t e, int64_t lo, int64_t hi, int64_t g0,
+                                              int64_t cur, int64_t cyc_start, float den) {
+  return glitch_ratio_of(glitch_pw(p, e, lo, hi, g0, cur, cyc_start), den);
 }
 
 // One work item of the walk: the cells order[order_begin + gblk * gates_per_block ...]
@@ -577,7 +591,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
           const bool prev_same = !((at_lo >> i) & 1) && sel<MAXP>(lt, i) >= cs_rel;
           const uint32_t nti = sel<MAXP>(nt, i);
           const bool next_same = nti == kRelBeyond || (nti != kRelInf && static_cast<int32_t>(nti) < ce_rel);
-          if (prev_same || next_same) {
+          if ((prev_same || next_same) && p.glitch_pw) {
+            const int64_t ev_idx = RING ? sel<MAXP>(f, i) - static_cast<int64_t>(sel<MAXP>(rs, i) >> 8) - 1
+                                        : sel<MAXP>(f, i) - 1;
+            g = glitch_ratio_of(__ldg(p.glitch_pw + ev_idx), __ldg(p.pin_gden + p0 + i));
+          } else if (prev_same || next_same) {
             const int32_t net = __ldg(p.pin_net + p0 + i);
             const int64_t lo = __ldg(p.net_off + net), hi = __ldg(p.net_off + net + 1);
             const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
@@ -800,6 +818,32 @@ __global__ void tile_first_kernel(const KParams pv, const KParams* __restrict__ 
   }
 }
 
+// ---- glitch pulse widths of every listed event ----
+
+// out[e] = glitch_pw of event e of its net, one warp per net. Parameters from
+// *pd when set (device memory), else from pv.
+__global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ pd, float* __restrict__ out) {
+  const KParams& p = pd ? *pd : pv;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t net = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; net < p.n_net;
+       net += warps) {
+    const int64_t lo = p.net_off[net], hi = p.net_off[net + 1];
+    if (lo < 0 || hi < lo || hi > p.n_event) continue;  // reported by the walk
+    const int64_t base = p.net_base ? p.net_base[net] : 0;
+    const int64_t g0 = base == 0 ? lo : -1;
+    for (int64_t e = lo + lane; e < hi; e += 32) {
+      const int64_t t = ev_time(p.ev_t, e);
+      const int64_t cyc = div_floor_pos(t, p.tpc, p.inv_tpc);
+      const int64_t cs = cyc * p.tpc;
+      // an event alone in its period is never a glitch event
+      const bool prev_same = e - 1 >= lo && ev_time(p.ev_t, e - 1) >= cs;
+      const bool next_same = e + 1 < hi && ev_time(p.ev_t, e + 1) < cs + p.tpc;
+      out[e] = (prev_same || next_same) ? glitch_pw(p, e, lo, hi, g0, t, cs) : -1.0f;
+    }
+  }
+}
+
 // ---- walk order by work ----
 
 __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
@@ -825,6 +869,14 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
 }
 
 }  // namespace
+
+cudaError_t launch_glitch_pw(const KParams& p, const KParams* d_p, float* out, cudaStream_t stream) {
+  if (p.n_net <= 0) return cudaSuccess;
+  const int64_t threads = static_cast<int64_t>(p.n_net) * 32;
+  const int blocks = static_cast<int>(std::min<int64_t>((threads + 255) / 256, 148 * 32));
+  glitch_pw_kernel<<<blocks, 256, 0, stream>>>(p, d_p, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_tile_first(const KParams& p, const KParams* d_p, int32_t* out, cudaStream_t stream) {
   const int64_t total = static_cast<int64_t>(p.n_tiles) * p.n_net;
