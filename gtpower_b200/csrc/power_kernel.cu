@@ -633,13 +633,14 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
           for (int q = 0; q < (MAXP < 2 ? 1 : MAXP - 1); ++q) {
             if (q >= n_in) break;
             if (!((has_wave >> q) & 1)) continue;
+            const int32_t tr = lt[q];
+            if (tr < cs_rel || tr >= ce_rel) continue;  // the related pin's edge lies in this cycle
             const bool fr = (last_rise >> q) & 1;
             const float dl = dlp[q * 4 + (fr ? 0 : 2)];
             if (isnan(dl)) continue;
-            const int32_t tr = lt[q];
             const double trs = __dmul_rn(static_cast<double>(T0 + tr), p.ts);
             const float diff = __double2float_rn(fabs(__dsub_rn(__dsub_rn(cur_s, static_cast<double>(dl)), trs)));
-            if (diff < best && tr >= cs_rel && tr < ce_rel) {
+            if (diff < best) {
               best = diff;
               relq = q;
               rel_rise = fr;
