@@ -112,6 +112,22 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, uint32_t lb
   return d.desc_;
 }
 
+// K-major operand in the 128-byte swizzle layout that a TMA box of 64 BF16
+// (128 bytes) x rows with CU_TENSOR_MAP_SWIZZLE_128B writes: rows 128 bytes
+// apart, 8-row groups 1024 bytes apart (sbo); the tile starts on a 1024-byte
+// boundary, and a K step inside the 128-byte row advances saddr by its bytes.
+__device__ __forceinline__ uint64_t smem_desc_kmajor_sw128(uint32_t saddr) {
+  cute::UMMA::SmemDescriptor d;
+  d.start_address_ = static_cast<uint16_t>((saddr >> 4) & 0x3FFF);
+  d.leading_byte_offset_ = 1;  // unused for swizzled K-major layouts
+  d.stride_byte_offset_ = static_cast<uint16_t>(1024 >> 4);
+  d.version_ = 1;
+  d.base_offset_ = 0;
+  d.lbo_mode_ = 0;
+  d.layout_type_ = static_cast<uint8_t>(cute::UMMA::LayoutType::SWIZZLE_128B);
+  return d.desc_;
+}
+
 // Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major.
 __host__ __device__ inline uint32_t instr_desc_bf16(int m, int n) {
   cute::UMMA::InstrDescriptor d;

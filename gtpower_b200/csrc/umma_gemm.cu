@@ -2,12 +2,11 @@
 //
 // One CTA computes a 128 x BN tile of C with 4 warps:
 //   warp 0, one lane : TMA producer. Per 64-wide K block it loads the A
-//                      tile (128 rows) and the B tile (BN rows) as eight
-//                      8-element (16-byte) column chunks each, so that shared
-//                      memory holds them in the K-major, no-swizzle canonical
-//                      layout: chunk c at c * rows * 16 bytes, row r of a
-//                      chunk at r * 16. Core matrices (8 rows x 16 bytes) are
-//                      then 128 bytes apart along M/N and rows*16 along K.
+//                      tile (128 rows) and the B tile (BN rows), one box of
+//                      64 BF16 (128 bytes) x rows each, with the 128-byte
+//                      swizzle: shared memory then holds them in the K-major
+//                      SWIZZLE_128B canonical layout (rows 128 bytes apart,
+//                      8-row groups 1024 bytes apart).
 //   warp 1, one lane : MMA issuer. Four tcgen05.mma (K = 16 each) per K
 //                      block into one TMEM accumulator of BN FP32 columns;
 //                      tcgen05.commit frees the stage for the producer.
@@ -28,9 +27,8 @@ namespace umma {
 namespace {
 
 constexpr int BM = 128, BK = 64, STAGES = 4, THREADS = 128;
-// Headroom after the last stage so that no descriptor of a stage can point
-// past the dynamic shared-memory allocation.
-constexpr int SLACK = 32 * 1024;
+// Guard after the last stage.
+constexpr int SLACK = 1024;
 
 template <int BN>
 struct Cfg {
@@ -122,11 +120,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint8_t* a = smem + s * C::STAGE;
         uint8_t* b = a + C::A_BYTES;
         tc::mbar_expect_tx(&full[s], C::STAGE);
-#pragma unroll
-        for (int c = 0; c < BK / 8; ++c) {
-          tc::tma_load_2d(a + c * (BM * 16), &tmA, &full[s], kb * BK + c * 8, m0);
-          tc::tma_load_2d(b + c * (BN * 16), &tmB, &full[s], kb * BK + c * 8, n0);
-        }
+        tc::tma_load_2d(a, &tmA, &full[s], kb * BK, m0);
+        tc::tma_load_2d(b, &tmB, &full[s], kb * BK, n0);
         issued = kb + 1;
       }
       if (*abort_v) {  // let this CTA's copies in flight land before exit
@@ -149,9 +144,9 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint32_t a = tc::smem_u32(smem + s * C::STAGE);
         const uint32_t b = a + C::A_BYTES;
 #pragma unroll
-        for (int j = 0; j < BK / 16; ++j) {
-          const uint64_t da = tc::smem_desc_kmajor(a + j * 2 * (BM * 16), BM * 16, 128);
-          const uint64_t db = tc::smem_desc_kmajor(b + j * 2 * (BN * 16), BN * 16, 128);
+        for (int j = 0; j < BK / 16; ++j) {  // K = 16 per MMA: 32 bytes along the swizzled row
+          const uint64_t da = tc::smem_desc_kmajor_sw128(a + j * 32);
+          const uint64_t db = tc::smem_desc_kmajor_sw128(b + j * 32);
           tc::umma_bf16(tmem, da, db, idesc, (kb | j) != 0 ? 1u : 0u);
         }
         tc::umma_commit(&empty[s]);
@@ -272,16 +267,16 @@ EncodeTiledFn encode_fn() {
 }
 
 // Tensor map over a row-major bf16 matrix [rows, ld] reading K columns, box
-// of 8 columns (16 bytes) by box_rows rows.
+// of 64 columns (128 bytes) by box_rows rows, 128-byte swizzle.
 bool make_map(CUtensorMap* map, const Operand& o, int64_t k, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (fn == nullptr) return false;
   const cuuint64_t dims[2] = {static_cast<cuuint64_t>(k), static_cast<cuuint64_t>(o.rows)};
   const cuuint64_t strides[1] = {static_cast<cuuint64_t>(o.ld) * 2};
-  const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t box[2] = {64, static_cast<cuuint32_t>(box_rows)};
   const cuuint32_t estr[2] = {1, 1};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(o.ptr), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -321,12 +316,13 @@ cudaError_t gemm_bf16_tn(const Operand& a, const Operand& b, int64_t m, int64_t 
     return cudaErrorInvalidValue;
   if ((ep.mode & EPI_BIAS) && ep.bias == nullptr) return cudaErrorInvalidValue;
   if ((ep.mode & EPI_COLSUM) && ep.colsum == nullptr) return cudaErrorInvalidValue;
-  if (bn == 0) bn = n <= 64 ? 64 : 128;
-  if (bn != 64 && bn != 128) return cudaErrorInvalidValue;
+  if (bn == 0) bn = n <= 64 ? 64 : (n <= 128 ? 128 : 256);
+  if (bn != 64 && bn != 128 && bn != 256) return cudaErrorInvalidValue;
   CUtensorMap ma, mb;
   if (!make_map(&ma, a, k, BM) || !make_map(&mb, b, k, bn)) return cudaErrorInvalidValue;
   if (bn == 64) return launch<64>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
-  return launch<128>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
+  if (bn == 128) return launch<128>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
+  return launch<256>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
 }
 
 }  // namespace umma

@@ -57,7 +57,7 @@ struct Operand {
 
 // Validates shapes and alignment (K % 8 == 0, ld % 8 == 0, 16-byte aligned
 // bases and vector stores) and launches. Returns cudaErrorInvalidValue on a
-// shape the kernel does not take. bn = 64 or 128 (0: by N).
+// shape the kernel does not take. bn = 64, 128 or 256 (0: by N).
 cudaError_t gemm_bf16_tn(const Operand& a, const Operand& b, int64_t m, int64_t n, int64_t k,
                          const Epilogue& ep, cudaStream_t stream, int bn = 0);
 
