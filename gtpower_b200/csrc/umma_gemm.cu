@@ -1,6 +1,6 @@
 // umma_gemm.cu — BF16 TN GEMM on tcgen05 with TMA-staged operands.
 //
-// One CTA computes a 128 x BN tile of C with 4 warps:
+// Persistent: one CTA per SM takes 128 x BN tiles of C in turn, with 6 warps:
 //   warp 0, one lane : TMA producer. Per 64-wide K block it loads the A
 //                      tile (128 rows) and the B tile (BN rows), one box of
 //                      64 BF16 (128 bytes) x rows each, with the 128-byte
@@ -8,11 +8,14 @@
 //                      SWIZZLE_128B canonical layout (rows 128 bytes apart,
 //                      8-row groups 1024 bytes apart).
 //   warp 1, one lane : MMA issuer. Four tcgen05.mma (K = 16 each) per K
-//                      block into one TMEM accumulator of BN FP32 columns;
-//                      tcgen05.commit frees the stage for the producer.
-//   warps 0-3        : epilogue. After the last commit every thread reads
-//                      its accumulator row (TMEM lane = tile row) 16 columns
-//                      at a time and applies the fused epilogue.
+//                      block into one of two TMEM accumulators of BN FP32
+//                      columns (alternating by tile); tcgen05.commit frees the
+//                      stage for the producer and, after a tile's last block,
+//                      hands the accumulator to the epilogue.
+//   warps 2-5        : epilogue. Warp w reads TMEM lanes (w % 4) * 32 .. +31
+//                      (the tile's rows) 16 columns at a time, applies the
+//                      fused epilogue and returns the accumulator, so that
+//                      the next tile's MMAs overlap this tile's stores.
 // A 4-stage ring of mbarriers (full: TMA bytes landed; empty: MMAs that read
 // the stage are done) overlaps loads with math. Every wait is bounded: on
 // timeout the kernel records an error bit, lets its own copies in flight
@@ -20,13 +23,16 @@
 #include "tc_sm100.cuh"
 #include "umma_gemm.h"
 
+#include <algorithm>
 #include <mutex>
 
 namespace gtpb {
 namespace umma {
 namespace {
 
-constexpr int BM = 128, BK = 64, STAGES = 4, THREADS = 128;
+constexpr int BM = 128, BK = 64, STAGES = 4;
+constexpr int EPI_WARPS = 4;                    // one per TMEM lane quarter
+constexpr int THREADS = 32 * (2 + EPI_WARPS);   // producer, MMA issuer, epilogue
 // Guard after the last stage.
 constexpr int SLACK = 1024;
 
@@ -37,7 +43,8 @@ struct Cfg {
   static constexpr int STAGE = A_BYTES + B_BYTES;
   static constexpr int TILES = STAGES * STAGE;
   static constexpr int SMEM = 1024 + TILES + SLACK + 256;
-  static constexpr uint32_t TMEM_COLS = BN;
+  static constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators: the epilogue of one tile
+                                                 // overlaps the MMAs of the next
 };
 
 __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float(static_cast<uint32_t>(b) << 16); }
@@ -79,13 +86,15 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::TILES + SLACK);
   uint64_t* empty = full + STAGES;
-  uint64_t* accb = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  uint64_t* acc_full = empty + STAGES;   // [2] accumulator ready for the epilogue
+  uint64_t* acc_empty = acc_full + 2;    // [2] accumulator drained by the epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   volatile int* abort_v = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const int nk = (K + BK - 1) / BK;
+  const int tiles_n = (N + BN - 1) / BN;
+  const int n_tiles = ((M + BM - 1) / BM) * tiles_n;
 
   if (threadIdx.x == 0) {
     tc::tma_prefetch_desc(&tmA);
@@ -94,11 +103,14 @@ __global__ void __launch_bounds__(THREADS, 1)
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    tc::mbar_init(accb, 1);
+    for (int a = 0; a < 2; ++a) {
+      tc::mbar_init(&acc_full[a], 1);
+      tc::mbar_init(&acc_empty[a], EPI_WARPS);
+    }
     *abort_v = 0;
     tc::mbar_init_fence();
   }
-  if (warp == 2) {
+  if (warp == 1) {
     tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
     tc::tmem_relinquish();
   }
@@ -108,142 +120,173 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
+    // TMA producer: one stage ring across all of this CTA's tiles
     if (lane == 0) {
-      int issued = 0;
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        if (kb >= STAGES && !tc::mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort_v)) {
-          *abort_v = 1;
-          if (ep.err) atomicOr(ep.err, 1);
-          break;
+      int64_t g = 0, issued = 0;
+      for (int t = blockIdx.x; t < n_tiles && !*abort_v; t += gridDim.x) {
+        const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = static_cast<int>(g % STAGES);
+          if (g >= STAGES && !tc::mbar_wait(&empty[s], static_cast<uint32_t>(((g / STAGES) - 1) & 1), abort_v)) {
+            *abort_v = 1;
+            if (ep.err) atomicOr(ep.err, 1);
+            break;
+          }
+          uint8_t* a = smem + s * C::STAGE;
+          uint8_t* b = a + C::A_BYTES;
+          tc::mbar_expect_tx(&full[s], C::STAGE);
+          tc::tma_load_2d(a, &tmA, &full[s], kb * BK, m0);
+          tc::tma_load_2d(b, &tmB, &full[s], kb * BK, n0);
+          issued = g + 1;
         }
-        uint8_t* a = smem + s * C::STAGE;
-        uint8_t* b = a + C::A_BYTES;
-        tc::mbar_expect_tx(&full[s], C::STAGE);
-        tc::tma_load_2d(a, &tmA, &full[s], kb * BK, m0);
-        tc::tma_load_2d(b, &tmB, &full[s], kb * BK, n0);
-        issued = kb + 1;
       }
       if (*abort_v) {  // let this CTA's copies in flight land before exit
-        for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
-          tc::mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, nullptr);
+        for (int64_t q = issued > STAGES ? issued - STAGES : 0; q < issued; ++q)
+          tc::mbar_wait(&full[q % STAGES], static_cast<uint32_t>((q / STAGES) & 1), nullptr);
       }
     }
     __syncwarp();
   } else if (warp == 1) {
+    // MMA issuer: accumulator i & 1 for this CTA's i-th tile
     if (lane == 0) {
       const uint32_t idesc = tc::instr_desc_bf16(BM, BN);
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        if (!tc::mbar_wait(&full[s], (kb / STAGES) & 1, abort_v)) {
+      int64_t g = 0;
+      int i = 0;
+      for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++i) {
+        const int acc = i & 1;
+        const uint32_t d = tmem + static_cast<uint32_t>(acc * BN);
+        bool ok = !*abort_v;
+        if (ok && i >= 2 && !tc::mbar_wait(&acc_empty[acc], static_cast<uint32_t>(((i / 2) - 1) & 1), abort_v))
+          ok = false;
+        for (int kb = 0; ok && kb < nk; ++kb, ++g) {
+          const int s = static_cast<int>(g % STAGES);
+          if (!tc::mbar_wait(&full[s], static_cast<uint32_t>((g / STAGES) & 1), abort_v)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t a = tc::smem_u32(smem + s * C::STAGE);
+          const uint32_t b = a + C::A_BYTES;
+#pragma unroll
+          for (int j = 0; j < BK / 16; ++j) {  // K = 16 per MMA: 32 bytes along the swizzled row
+            const uint64_t da = tc::smem_desc_kmajor_sw128(a + j * 32);
+            const uint64_t db = tc::smem_desc_kmajor_sw128(b + j * 32);
+            tc::umma_bf16(d, da, db, idesc, (kb | j) != 0 ? 1u : 0u);
+          }
+          tc::umma_commit(&empty[s]);
+        }
+        tc::umma_commit(&acc_full[acc]);  // arrives once every MMA issued so far is done
+        if (!ok) {
           *abort_v = 1;
           if (ep.err) atomicOr(ep.err, 1);
           break;
         }
-        tc::tc_fence_after();
-        const uint32_t a = tc::smem_u32(smem + s * C::STAGE);
-        const uint32_t b = a + C::A_BYTES;
-#pragma unroll
-        for (int j = 0; j < BK / 16; ++j) {  // K = 16 per MMA: 32 bytes along the swizzled row
-          const uint64_t da = tc::smem_desc_kmajor_sw128(a + j * 32);
-          const uint64_t db = tc::smem_desc_kmajor_sw128(b + j * 32);
-          tc::umma_bf16(tmem, da, db, idesc, (kb | j) != 0 ? 1u : 0u);
-        }
-        tc::umma_commit(&empty[s]);
       }
-      tc::umma_commit(accb);  // arrives once every MMA issued above is done
     }
     __syncwarp();
-  }
-
-  // ---- epilogue (all four warps) -------------------------------------------
-  int acc_ok = 1;
-  if (lane == 0) acc_ok = tc::mbar_wait(accb, 0, nullptr) ? 1 : 0;
-  acc_ok = __shfl_sync(0xffffffffu, acc_ok, 0);
-  tc::tc_fence_after();
-  if (!acc_ok) {
-    if (lane == 0 && ep.err) atomicOr(ep.err, 1);
-  } else if (!*abort_v) {
-    const int mode = ep.mode;
-    const int row = m0 + warp * 32 + lane;
-    const bool row_ok = row < M;
-    const uint32_t lane_base = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-    const uint16_t* mrow = static_cast<const uint16_t*>(ep.mask) + static_cast<int64_t>(row) * ep.ldm;
-    float sq = 0.f;
-    for (int c = 0; c < BN; c += 16) {
-      const int nb = n0 + c;
-      if (nb >= N) break;
-      float v[16];
-      tc::tmem_ld16(lane_base + static_cast<uint32_t>(c), v);
-      float mk[16];
-      if (mode & EPI_RELU_BWD) {
-        if (row_ok) load16_bf16(mrow, nb, N, true, mk);
-        else {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) mk[j] = 0.f;
-        }
+  } else {
+    // epilogue warps: warp w reads TMEM lanes (w % 4) * 32 ..., i.e. tile rows
+    const int quarter = warp & 3;
+    int i = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++i) {
+      const int acc = i & 1;
+      int acc_ok = 1;
+      if (lane == 0) acc_ok = tc::mbar_wait(&acc_full[acc], static_cast<uint32_t>((i / 2) & 1), nullptr) ? 1 : 0;
+      acc_ok = __shfl_sync(0xffffffffu, acc_ok, 0);
+      tc::tc_fence_after();
+      if (!acc_ok) {
+        if (lane == 0 && ep.err) atomicOr(ep.err, 1);
+        break;
       }
+      if (*abort_v) break;
+      const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+      const int mode = ep.mode;
+      const int row = m0 + quarter * 32 + lane;
+      const bool row_ok = row < M;
+      const uint32_t lane_base = tmem + static_cast<uint32_t>(acc * BN) + (static_cast<uint32_t>(quarter * 32) << 16);
+      const uint16_t* mrow = static_cast<const uint16_t*>(ep.mask) + static_cast<int64_t>(row) * ep.ldm;
+      float sq = 0.f;
+      for (int c = 0; c < BN; c += 16) {
+        const int nb = n0 + c;
+        if (nb >= N) break;
+        float v[16];
+        tc::tmem_ld16(lane_base + static_cast<uint32_t>(c), v);
+        float mk[16];
+        if (mode & EPI_RELU_BWD) {
+          if (row_ok) load16_bf16(mrow, nb, N, true, mk);
+          else {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = nb + j;
-        const bool ok = row_ok && n < N;
-        float x = v[j];
-        if (mode & EPI_BIAS) x += (n < N) ? ep.bias[n] : 0.f;
-        if (mode & EPI_RELU) x = fmaxf(x, 0.f);
-        if (mode & EPI_RELU_BWD) x = mk[j] > 0.f ? x : 0.f;
-        if (mode & EPI_MSE) {
-          if (ok && (mode & EPI_OUT_F32)) ep.out_f[static_cast<int64_t>(row) * ep.ldf + n] = x;
-          float g = 0.f;
-          if (ok && n < ep.n_valid) {
-            g = x - ep.target[static_cast<int64_t>(row) * ep.ldy + n];
-            sq += g * g;
+            for (int j = 0; j < 16; ++j) mk[j] = 0.f;
           }
-          x = g * ep.grad_scale;
-        } else if (ok && (mode & EPI_OUT_F32)) {
-          ep.out_f[static_cast<int64_t>(row) * ep.ldf + n] = x;
         }
-        v[j] = ok ? x : 0.f;
-      }
-      if ((mode & EPI_OUT_BF16) && row_ok) {
-        uint16_t* orow = static_cast<uint16_t*>(ep.out) + static_cast<int64_t>(row) * ep.ldo;
-        if (nb + 16 <= N) {
-          uint4 q0, q1;
-          q0.x = pack2(v[0], v[1]);
-          q0.y = pack2(v[2], v[3]);
-          q0.z = pack2(v[4], v[5]);
-          q0.w = pack2(v[6], v[7]);
-          q1.x = pack2(v[8], v[9]);
-          q1.y = pack2(v[10], v[11]);
-          q1.z = pack2(v[12], v[13]);
-          q1.w = pack2(v[14], v[15]);
-          *reinterpret_cast<uint4*>(orow + nb) = q0;
-          *reinterpret_cast<uint4*>(orow + nb + 8) = q1;
-        } else {
-          for (int j = 0; j < 16 && nb + j < N; ++j) orow[nb + j] = f2bf(v[j]);
-        }
-      }
-      if ((mode & EPI_OUT_BF16_T) && row_ok) {
-        uint16_t* ot = static_cast<uint16_t*>(ep.out_t);
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (nb + j < N) ot[static_cast<int64_t>(nb + j) * ep.ldt + row] = f2bf(v[j]);
-      }
-      if (mode & EPI_COLSUM) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const float s = warp_sum(v[j]);
-          if (lane == 0 && nb + j < N) atomicAdd(&ep.colsum[nb + j], s);
+          const int n = nb + j;
+          const bool ok = row_ok && n < N;
+          float x = v[j];
+          if (mode & EPI_BIAS) x += (n < N) ? ep.bias[n] : 0.f;
+          if (mode & EPI_RELU) x = fmaxf(x, 0.f);
+          if (mode & EPI_RELU_BWD) x = mk[j] > 0.f ? x : 0.f;
+          if (mode & EPI_MSE) {
+            if (ok && (mode & EPI_OUT_F32)) ep.out_f[static_cast<int64_t>(row) * ep.ldf + n] = x;
+            float g = 0.f;
+            if (ok && n < ep.n_valid) {
+              g = x - ep.target[static_cast<int64_t>(row) * ep.ldy + n];
+              sq += g * g;
+            }
+            x = g * ep.grad_scale;
+          } else if (ok && (mode & EPI_OUT_F32)) {
+            ep.out_f[static_cast<int64_t>(row) * ep.ldf + n] = x;
+          }
+          v[j] = ok ? x : 0.f;
+        }
+        if ((mode & EPI_OUT_BF16) && row_ok) {
+          uint16_t* orow = static_cast<uint16_t*>(ep.out) + static_cast<int64_t>(row) * ep.ldo;
+          if (nb + 16 <= N) {
+            uint4 q0, q1;
+            q0.x = pack2(v[0], v[1]);
+            q0.y = pack2(v[2], v[3]);
+            q0.z = pack2(v[4], v[5]);
+            q0.w = pack2(v[6], v[7]);
+            q1.x = pack2(v[8], v[9]);
+            q1.y = pack2(v[10], v[11]);
+            q1.z = pack2(v[12], v[13]);
+            q1.w = pack2(v[14], v[15]);
+            *reinterpret_cast<uint4*>(orow + nb) = q0;
+            *reinterpret_cast<uint4*>(orow + nb + 8) = q1;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (nb + j < N) orow[nb + j] = f2bf(v[j]);
+          }
+        }
+        if ((mode & EPI_OUT_BF16_T) && row_ok) {
+          uint16_t* ot = static_cast<uint16_t*>(ep.out_t);
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < N) ot[static_cast<int64_t>(nb + j) * ep.ldt + row] = f2bf(v[j]);
+        }
+        if (mode & EPI_COLSUM) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float s = warp_sum(v[j]);
+            if (lane == 0 && nb + j < N) atomicAdd(&ep.colsum[nb + j], s);
+          }
         }
       }
-    }
-    if (mode & EPI_MSE) {
-      sq = warp_sum(sq);
-      if (lane == 0 && ep.loss) atomicAdd(ep.loss, sq);
+      if (mode & EPI_MSE) {
+        sq = warp_sum(sq);
+        if (lane == 0 && ep.loss) atomicAdd(ep.loss, sq);
+      }
+      // hand the accumulator back to the MMA issuer
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&acc_empty[acc]);
     }
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 2) {
+  if (warp == 1) {
     tc::tc_fence_after();
     tc::tmem_dealloc(tmem, C::TMEM_COLS);
   }
@@ -292,7 +335,14 @@ cudaError_t launch(const CUtensorMap& ma, const CUtensorMap& mb, int m, int n, i
     attr = cudaFuncSetAttribute(gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
   });
   if (attr != cudaSuccess) return attr;
-  const dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM);
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const int64_t tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+  const int grid = static_cast<int>(std::min<int64_t>(tiles, sms));  // persistent: one CTA per SM
   gemm_kernel<BN><<<grid, THREADS, C::SMEM, stream>>>(ma, mb, m, n, k, ep);
   return cudaGetLastError();
 }
