@@ -29,6 +29,7 @@ struct gtp_ctx {
   int32_t *d_cell_pin_off = nullptr, *d_cell_type = nullptr, *d_cell_inst = nullptr,
           *d_order = nullptr, *d_pin_net = nullptr, *d_pin_slot = nullptr;
   uint8_t *d_pin_flags = nullptr, *d_cell_group = nullptr;
+  uint8_t* d_net_glitch = nullptr;  // [n_net] 1 when some non-clock pin reads the net
   float *d_pin_gden = nullptr, *d_pin_swe = nullptr, *d_leak_pool = nullptr, *d_inst = nullptr;
   DevType* d_types = nullptr;
   DevSlot* d_slots = nullptr;
@@ -110,7 +111,7 @@ double fixed_point_scale(double bound) {
 
 void free_all(gtp_ctx* c) {
   void* ptrs[] = {c->d_cell_pin_off, c->d_cell_type, c->d_cell_inst, c->d_order, c->d_pin_net,
-                  c->d_pin_slot, c->d_pin_flags, c->d_cell_group, c->d_pin_gden, c->d_pin_swe,
+                  c->d_pin_slot, c->d_pin_flags, c->d_cell_group, c->d_pin_gden, c->d_pin_swe, c->d_net_glitch,
                   c->d_leak_pool, c->d_inst, c->d_types, c->d_slots, c->d_cubes,
                   c->slot[0].d_net_off, c->slot[0].d_ev_t, c->slot[0].d_net_base, c->slot[0].d_ev_v,
                   c->slot[1].d_net_off, c->slot[1].d_ev_t, c->slot[1].d_net_base, c->slot[1].d_ev_v,
@@ -138,6 +139,7 @@ KParams make_params(gtp_ctx* c) {
   k.order = c->d_order;
   k.pin_net = c->d_pin_net;
   k.pin_flags = c->d_pin_flags;
+  k.net_glitch = c->d_net_glitch;
   k.pin_gden = c->d_pin_gden;
   k.pin_swe = c->d_pin_swe;
   k.types = c->d_types;
@@ -391,6 +393,13 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
   UP(d_pin_net, P.pin_net);
   UP(d_pin_slot, P.pin_slot);
   UP(d_pin_flags, P.pin_flags);
+  {
+    // nets read by some non-clock pin: only those need glitch widths
+    std::vector<uint8_t> ng(std::max(1, P.n_net), 0);
+    for (size_t q = 0; q < P.pin_net.size(); ++q)
+      if (P.pin_net[q] >= 0 && P.pin_net[q] < P.n_net && !(P.pin_flags[q] & 4)) ng[P.pin_net[q]] = 1;
+    UP(d_net_glitch, ng);
+  }
   UP(d_cell_group, P.cell_group);
   UP(d_pin_gden, P.pin_gden);
   UP(d_pin_swe, P.pin_swe);

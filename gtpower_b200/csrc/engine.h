@@ -115,6 +115,7 @@ struct KParams {
   int32_t order_begin, order_end;
   const int32_t* pin_net;
   const uint8_t* pin_flags;
+  const uint8_t* net_glitch;        // [n_net] 1 when some non-clock pin reads the net, or null
   const float* pin_gden;
   const float* pin_swe;
   const DevType* types;

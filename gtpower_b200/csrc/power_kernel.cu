@@ -831,6 +831,7 @@ __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ p
        net += warps) {
     const int64_t lo = p.net_off[net], hi = p.net_off[net + 1];
     if (lo < 0 || hi < lo || hi > p.n_event) continue;  // reported by the walk
+    if (p.net_glitch && !p.net_glitch[net]) continue;   // read by clock pins only: never a glitch
     const int64_t base = p.net_base ? p.net_base[net] : 0;
     const int64_t g0 = base == 0 ? lo : -1;
     for (int64_t e = lo + lane; e < hi; e += 32) {
