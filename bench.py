@@ -51,6 +51,8 @@ def parse():
                          "(with their context), so that each window's copy overlaps the previous walk")
     ap.add_argument("--gates-per-block", type=int, default=0)
     ap.add_argument("--threads-per-block", type=int, default=0)
+    ap.add_argument("--no-clock-runs", action="store_true",
+                    help="walk periodic clock pins edge by edge instead of as runs of whole cycles")
     ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream"],
                     help="flat: the plain walk (default); proxy: the learned per-cycle power proxy "
                          "against the plain walk on a phased-unit trace; batch: 64 uneven traces x "
@@ -628,7 +630,8 @@ def main():
         h2d = 8 * (design.n_net + 1) + 8 * n_event + 4 * ((n_event + 15) // 16)
 
     eng = B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
-                    gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block)
+                    gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
+                    clock_runs=not args.no_clock_runs)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     def device_step():
@@ -727,6 +730,7 @@ def main():
                        "cell_cycles_per_s": world * design.n_cell * eng.n_period / (step_ms / 1e3),
                        "l2": "inputs larger than L2 (event CSR %.2f GB)" % (h2d / 1e9),
                        "walk_ms": walk_ms, "generation_s": gen_s,
+                       "clock_pins": "edge by edge" if args.no_clock_runs else "runs of whole cycles when periodic",
                        "parallelism": f"weak: {world} independent traces" if world > 1 else "1 GPU"},
             "e2e": {"value": world * n_event / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,

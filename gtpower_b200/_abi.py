@@ -85,7 +85,7 @@ class gtp_config(C.Structure):
                 ("n_thread_per_block", C.c_int32), ("gates_per_block", C.c_int32),
                 ("max_n_pin_for_leakage_power", C.c_int32), ("collect_counts", C.c_int32),
                 ("max_event_num", C.c_int64), ("sort_by_work", C.c_int32),
-                ("reserved32", C.c_int32), ("reserved", C.c_int64 * 3)]
+                ("clock_runs", C.c_int32), ("reserved", C.c_int64 * 3)]
 
 
 class gtp_counts(C.Structure):
@@ -112,7 +112,7 @@ EXPORTED = sorted([
     "gtp_ticks_per_cycle", "gtp_reset", "gtp_push_events", "gtp_push_events_device",
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
     "gtp_evaluate_noalloc", "gtp_pack_values",
-    "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups",
+    "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups", "gtp_clock_run_nets",
     "gtp_batch_config_default", "gtp_batch_create", "gtp_batch_destroy", "gtp_batch_last_error",
     "gtp_batch_push_device", "gtp_batch_sync", "gtp_batch_get_stream", "gtp_batch_stats",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
@@ -177,6 +177,8 @@ def lib() -> C.CDLL:
     L.gtp_n_cycle_groups.restype = C.c_int32
     L.gtp_fetch_cycle_groups.argtypes = [C.c_void_p, _P]
     L.gtp_fetch_cycle_groups.restype = C.c_int32
+    L.gtp_clock_run_nets.argtypes = [C.c_void_p, _P, _P]
+    L.gtp_clock_run_nets.restype = C.c_int32
     _bind_proxy(L)
     _lib = L
     return L

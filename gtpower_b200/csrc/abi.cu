@@ -30,6 +30,11 @@ struct gtp_ctx {
           *d_order = nullptr, *d_pin_net = nullptr, *d_pin_slot = nullptr;
   uint8_t *d_pin_flags = nullptr, *d_cell_group = nullptr;
   uint8_t* d_net_glitch = nullptr;  // [n_net] 1 when some non-clock pin reads the net
+  // nets read by clock pins, and their per-window periodic patterns
+  int32_t* d_clk_nets = nullptr;
+  int32_t n_clk_nets = 0;
+  std::vector<int32_t> clk_nets;
+  int2* d_pclk = nullptr;            // [n_net]
   float *d_pin_gden = nullptr, *d_pin_swe = nullptr, *d_leak_pool = nullptr, *d_inst = nullptr;
   DevType* d_types = nullptr;
   DevSlot* d_slots = nullptr;
@@ -119,7 +124,7 @@ void free_all(gtp_ctx* c) {
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
-                  c->d_cycle5_g, c->d_leak_tmp_g};
+                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& sl : c->slot)
@@ -184,10 +189,18 @@ KParams make_params(gtp_ctx* c) {
 }
 
 // Largest cycle tile whose shared memory (bins with counters, event
-// buffers, tables) stays within 227 KB.
-int64_t max_cycles_per_tile(int threads, int bin_sets) {
-  const int64_t budget = 227 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4));
-  return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (bin_sets * kNumCycAcc * 8 + 8)));
+// buffers, tables, and 1 KB for the walk's static shared memory) stays
+// within 227 KB.
+int64_t max_cycles_per_tile(int threads, int bin_sets, bool clock_runs = false) {
+  const int64_t budget = 226 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4));
+  const int slots = clock_runs ? kNumBinSlotsRun : kNumCycAcc;
+  return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (bin_sets * slots * 8 + 8)));
+}
+
+// Whether windows of this context walk periodic clock pins as runs.
+bool clock_runs_on(const gtp_ctx* c) {
+  return c->cfg.clock_runs >= 0 && c->n_clk_nets > 0 && c->d_pclk && !c->P.drift && c->P.tpc >= 2 &&
+         c->P.tpc < (int64_t(1) << 30);
 }
 
 // Validates one window and sets up its walk parameters *out (sorting the
@@ -223,7 +236,8 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   // bins + event buffers + tables within 227 KB of shared memory; tile span
   // (ct+1)*tpc within 2^31 ticks, as the walk holds times as 32-bit offsets
   // from the tile start
-  const int64_t max_ct = std::min<int64_t>(max_cycles_per_tile(threads_, c->n_cgroup > 0 ? 2 : 1),
+  const bool runs = clock_runs_on(c);
+  const int64_t max_ct = std::min<int64_t>(max_cycles_per_tile(threads_, c->n_cgroup > 0 ? 2 : 1, runs),
                                            (int64_t(INT32_MAX) / P.tpc) - 1);
   ct = std::min(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);  // grid.y limit
@@ -264,10 +278,12 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     if (c->d_glitch_pw) k.glitch_pw = c->d_glitch_pw;
   }
   if (c->cfg.sort_by_work && c->d_order_work) k.order = c->d_order_work;
+  if (runs) k.pclk = c->d_pclk;
   if (enqueue_prep) {
     cudaError_t e = cudaSuccess;
     if (k.tile_first) e = launch_tile_first(k, nullptr, c->d_tile_first, stream);
     if (e == cudaSuccess && k.glitch_pw) e = launch_glitch_pw(k, nullptr, c->d_glitch_pw, stream);
+    if (e == cudaSuccess && k.pclk) e = launch_pclk(k, nullptr, c->d_clk_nets, c->n_clk_nets, c->d_pclk, stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tile index");
     if (c->cfg.sort_by_work && c->d_order_work) {
       e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
@@ -288,6 +304,10 @@ cudaError_t enqueue_window_prep(gtp_ctx* c, const KParams& k, const KParams* d_k
   }
   if (k.glitch_pw) {
     cudaError_t e = launch_glitch_pw(k, d_k, c->d_glitch_pw, stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (k.pclk) {
+    cudaError_t e = launch_pclk(k, d_k, c->d_clk_nets, c->n_clk_nets, c->d_pclk, stream);
     if (e != cudaSuccess) return e;
   }
   if (!(c->cfg.sort_by_work && c->d_order_work)) return cudaSuccess;
@@ -399,6 +419,19 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     for (size_t q = 0; q < P.pin_net.size(); ++q)
       if (P.pin_net[q] >= 0 && P.pin_net[q] < P.n_net && !(P.pin_flags[q] & 4)) ng[P.pin_net[q]] = 1;
     UP(d_net_glitch, ng);
+    // nets read by clock pins: candidates for periodic patterns
+    std::vector<uint8_t> isclk(std::max(1, P.n_net), 0);
+    for (size_t q = 0; q < P.pin_net.size(); ++q)
+      if (P.pin_net[q] >= 0 && P.pin_net[q] < P.n_net && (P.pin_flags[q] & 4)) isclk[P.pin_net[q]] = 1;
+    for (int32_t n = 0; n < P.n_net; ++n)
+      if (isclk[n]) c->clk_nets.push_back(n);
+    c->n_clk_nets = static_cast<int32_t>(c->clk_nets.size());
+    if (c->n_clk_nets > 0) {
+      UP(d_clk_nets, c->clk_nets);
+      e = cudaMalloc(&c->d_pclk, sizeof(int2) * static_cast<size_t>(P.n_net));
+      if (e == cudaSuccess) e = cudaMemsetAsync(c->d_pclk, 0xff, sizeof(int2) * static_cast<size_t>(P.n_net), c->stream);
+      if (e != cudaSuccess) goto cuda_err;
+    }
   }
   UP(d_cell_group, P.cell_group);
   UP(d_pin_gden, P.pin_gden);
@@ -710,6 +743,22 @@ gtp_status gtp_set_cycle_groups(gtp_ctx* c, const int32_t* cell_group, int32_t n
 
 int32_t gtp_n_cycle_groups(const gtp_ctx* c) { return c ? c->n_cgroup : 0; }
 
+gtp_status gtp_clock_run_nets(gtp_ctx* c, int32_t* n_clock_nets, int32_t* n_periodic) {
+  if (!c || !n_clock_nets || !n_periodic) return GTP_EINVAL;
+  *n_clock_nets = c->n_clk_nets;
+  *n_periodic = 0;
+  if (c->n_clk_nets == 0 || !c->d_pclk) return GTP_OK;
+  std::vector<int2> tab(static_cast<size_t>(c->P.n_net));
+  cudaError_t e = cudaMemcpyAsync(tab.data(), c->d_pclk, sizeof(int2) * tab.size(), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "gtp_clock_run_nets");
+  int32_t n = 0;
+  for (int32_t net : c->clk_nets)
+    if (tab[static_cast<size_t>(net)].x >= 0) ++n;
+  *n_periodic = n;
+  return GTP_OK;
+}
+
 gtp_status gtp_fetch_cycle_groups(gtp_ctx* c, float* cycle5_groups) {
   if (!c || !cycle5_groups) return GTP_EINVAL;
   if (c->n_cgroup <= 0) {
@@ -920,9 +969,11 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
   struct Item { double w; int4 v; };
   std::vector<std::vector<Item>> groups(kBatchGroups);
   size_t smem_g[kBatchGroups] = {0, 0, 0, 0, 0, 0};
+  bool runs_g[kBatchGroups] = {false, false, false, false, false, false};
   for (size_t q = 0; q < entries.size(); ++q) {
     const BatchEntry& be = entries[q];
     const int bk = be.group / 2;
+    if (bk == 0 && !(be.group & 1) && params[q].pclk) runs_g[be.group] = true;
     smem_g[be.group] = std::max(smem_g[be.group], walk_item_smem_bytes(params[q], bucket_pins[bk], b->counts, b->threads));
     for (int g = 0; g < be.n_gblk; ++g) {
       const int32_t cells = std::min<int32_t>(be.gpb, be.cells - g * be.gpb);
@@ -1015,8 +1066,8 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     for (int g = 0; g < kBatchGroups; ++g) {
       if (!grid_g[g]) continue;
       r = launch_power_walk_batch(b->d_params, b->d_items + group_off[g], b->d_meta + 2 * g, b->d_meta + 2 * g + 1,
-                                  grid_g[g], bucket_pins[g / 2], b->counts, (g & 1) != 0, b->threads, smem_g[g],
-                                  b->stream);
+                                  grid_g[g], bucket_pins[g / 2], b->counts, (g & 1) != 0, runs_g[g], b->threads,
+                                  smem_g[g], b->stream);
       if (r != cudaSuccess) return r;
     }
     return r;

@@ -64,6 +64,9 @@ struct DevSlot {
 constexpr int kMaxPins = 32;      // cell pins supported by the walk
 constexpr int kFastPins = 4;      // cells up to this many pins use fast_tab
 constexpr int kNumCycAcc = 6;     // per-cycle fixed-point accumulators
+constexpr int kNumBinSlotsRun = 8; // shared-memory bin slots per set with clock runs:
+                                   // the 6 above, then run-differences of the
+                                   // per-cycle clock-edge internal energy and leakage
 constexpr int kNumCellAcc = 5;
 
 // Host-side packed design.
@@ -139,6 +142,11 @@ struct KParams {
                              // relative to net_off; null: the walk bisects
   const float* glitch_pw;    // [n_event] glitch pulse width (s) of each listed event, -1 when
                              // not a glitch event; null: the walk classifies
+  const int2* pclk;          // [n_net] for nets read by clock pins: the window's periodic
+                             // pattern (x: phase of the cycle's first edge in ticks, -1 =
+                             // not periodic; y: phase of the second edge | 1 << 30 when
+                             // the edge at time_max is absent | value at the cycle start
+                             // << 31); null: every clock edge is walked
   int64_t n_event;
   int64_t t_lo, t_hi;
   int32_t n_net;
@@ -197,17 +205,27 @@ cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int t
 // (x: params index, y: gate block, z: tile), *d_n_items their count and
 // *d_counter the queue head (zeroed before the launch). smem must cover the
 // largest item's shared memory.
+// runs: the launch walks periodic clock pins as runs (items whose p.pclk is
+// set; fast bucket without drift only).
 cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items, const int* d_n_items,
-                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, int threads,
-                                    size_t smem, cudaStream_t stream);
+                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, bool runs,
+                                    int threads, size_t smem, cudaStream_t stream);
 // Dynamic shared memory of one walk block for these parameters.
 size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int threads);
 // Resident blocks per SM of the persistent walk at this shape.
 int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem);
 
-// bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group.
+// bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group;
+// clock_runs: the bins carry the two clock-run slots (p.pclk set).
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
-                             size_t tab_bytes, int bin_sets = 1);
+                             size_t tab_bytes, int bin_sets = 1, bool clock_runs = false);
+
+// Fills the pattern table p.pclk (`out`) for the n nets in `nets` over the
+// window p describes: a net is periodic when its events in [max(t_lo, 1),
+// min(t_hi, tmax + 1)) are exactly one edge at phase x and one at phase y of
+// every cycle, alternating between 0 and 1, with a known value before them.
+cudaError_t launch_pclk(const KParams& p, const KParams* d_p, const int32_t* nets, int32_t n, int2* out,
+                        cudaStream_t stream);
 
 // Fills p.glitch_pw's array (`out`, n_event entries) for the window p
 // describes; with d_p set the kernel reads the window from there.

@@ -130,6 +130,9 @@ struct Bins {
 constexpr int kLeakPart = 0;   // leakage inside the cycle of each change
 constexpr int kLeakLevel = 1;  // run-difference of the per-cycle leakage level
 constexpr int kInt = 2, kGInt = 3, kSw = 4, kGSw = 5;
+// shared-memory slots of the clock runs (tile-local run-differences, prefix
+// summed into kInt and kLeakPart when the tile is flushed)
+constexpr int kIntRun = 6, kLeakRun = 7;
 
 __device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, int64_t c,
                                         unsigned long long x) {
@@ -153,6 +156,40 @@ __device__ __forceinline__ void add_cnt(const KParams& p, const Bins& b, int q, 
     const int64_t cc = c < p.n_period ? c : p.n_period;
     atomicAdd(p.cnt_cyc + q * (p.n_period + 1) + cc, 1ull);
   }
+}
+
+// In-place inclusive prefix sum of a[0, n) in shared memory, by all threads
+// of the block (blockDim.x a multiple of 32); wsum: 32 words of scratch.
+__device__ void block_inclusive_scan(unsigned long long* a, int64_t n, unsigned long long* wsum) {
+  const int nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int64_t chunk = (n + nt - 1) / nt;
+  const int64_t lo = min(n, static_cast<int64_t>(tid) * chunk), hi = min(n, lo + chunk);
+  unsigned long long s = 0;
+  for (int64_t k = lo; k < hi; ++k) {
+    s += a[k];
+    a[k] = s;
+  }
+  unsigned long long x = s;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long v = lane < (nt >> 5) ? wsum[lane] : 0ull;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, v, d);
+      if (lane >= d) v += y;
+    }
+    wsum[lane] = v;
+  }
+  __syncthreads();
+  const unsigned long long off = (x - s) + (w > 0 ? wsum[w - 1] : 0ull);
+  for (int64_t k = lo; k < hi; ++k) a[k] += off;
+  __syncthreads();
 }
 
 // Seconds cycle of tick t: the largest c with c*period <= t*ts (the
@@ -248,27 +285,33 @@ __device__ __forceinline__ float glitch_ratio(const KParams& p, int64_t e, int64
 // One work item of the walk: the cells order[order_begin + gblk * gates_per_block ...]
 // of one pin bucket over cycle tile `tile` of the window, with the block's
 // dynamic shared memory `smem`. All threads of the block call it together.
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile,
                                            unsigned long long* smem) {
   const int64_t ct = p.cycles_per_tile;
   // per-cycle groups: two bin sets, for the block's first group and the next
   const int nset = p.cell_cgroup ? 2 : 1;
+  // periodic clock pins (RUNS: cells of up to kFastPins pins, no drift):
+  // each set carries the two clock-run slots
+  static_assert(!RUNS || (FAST && !DRIFT), "clock runs need the fast walk without drift");
+  const bool runs_on = RUNS && p.pclk != nullptr;
+  const int nslot = runs_on ? kNumBinSlotsRun : kNumCycAcc;
+  __shared__ unsigned long long s_wsum[32];
   Bins bins;
   bins.s = smem;
-  bins.sc = reinterpret_cast<uint32_t*>(smem + nset * kNumCycAcc * ct);
+  bins.sc = reinterpret_cast<uint32_t*>(smem + nset * nslot * ct);
   bins.off = 0;
   bins.g = 0;
   bins.c_lo = p.cyc0 + static_cast<int64_t>(tile) * ct;
   bins.ct = ct;
-  for (int64_t k = threadIdx.x; k < nset * kNumCycAcc * ct; k += blockDim.x) smem[k] = 0ull;
+  for (int64_t k = threadIdx.x; k < nset * nslot * ct; k += blockDim.x) smem[k] = 0ull;
   if (COUNTS)
     for (int64_t k = threadIdx.x; k < 2 * ct; k += blockDim.x) bins.sc[k] = 0u;
   // RING: per-thread event buffers [pin][slot][thread] of times - T0, then
   // the per-type energy-selection and leakage tables when they fit
   constexpr bool RING = FAST && WALK_USE_RING;
   constexpr bool STAGE = FAST && WALK_STAGE_INST;
-  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + nset * kNumCycAcc * ct + (COUNTS ? ct : 0));
+  uint32_t* ring = reinterpret_cast<uint32_t*>(smem + nset * nslot * ct + (COUNTS ? ct : 0));
   const int nt_blk = blockDim.x;
   const int16_t* fast_tab = p.fast_tab;
   const float* leak_pool = p.leak_pool;
@@ -296,6 +339,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   const uint32_t span = static_cast<uint32_t>(T1 > T0 ? T1 - T0 : 0);
   const bool owns_initial = (tile == 0) && (p.t_lo == 0);
   const double P = p.period_d;
+  // clock runs: a periodic pin's edges exist from tick max(t_lo, 1) on
+  // (r_exist relative to T0); the tile holds those before span
+  int32_t r_exist = 0;
+  if (runs_on) {
+    const int64_t tl = max(p.t_lo, static_cast<int64_t>(1)) - T0;
+    r_exist = static_cast<int32_t>(max(tl, -static_cast<int64_t>(INT32_MAX / 2)));
+  }
 
   const int32_t g_begin = p.order_begin + gblk * p.gates_per_block;
   const int32_t g_end = min(p.order_end, g_begin + p.gates_per_block);
@@ -308,7 +358,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     if (p.cell_cgroup) {
       bins.g = __ldg(p.cell_cgroup + cell);
       const int32_t set = bins.g - g_first;
-      bins.off = (set == 0 || set == 1) ? static_cast<int64_t>(set) * kNumCycAcc * ct : -1;
+      bins.off = (set == 0 || set == 1) ? static_cast<int64_t>(set) * nslot * ct : -1;
     }
     const int32_t p0 = __ldg(p.cell_pin_off + cell);
     const int32_t type = __ldg(p.cell_type + cell);
@@ -326,6 +376,26 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       }
     }
     const float* blk = STAGE ? s_inst : blk_g;
+    // internal energy of input pin i's event (before the rise/fall and
+    // toggle factors) under the pre-step pin values oo
+    auto in_energy = [&](int i, uint32_t oo, bool rise) -> float {
+      float en = 0.0f;
+      if (FAST) {
+        const int16_t eo = fast_tab[fo + i * n_state + oo];
+        if (eo >= 0) en = blk[eo + (rise ? 0 : 1)];
+      } else {
+        const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + i);
+        const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + i + 1);
+        for (int32_t k = s_begin; k < s_end; ++k) {
+          const DevSlot sl = p.slots[k];
+          if (when_holds(p.cubes, sl.cube_off, sl.n_cube, oo)) {
+            en = blk[sl.e_off + (rise ? 0 : 1)];
+            break;
+          }
+        }
+      }
+      return en;
+    };
 
     int64_t f[MAXP];          // next event index to read (absolute)
     int32_t rem[MAXP];        // events left to read in the accessible range
@@ -339,6 +409,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     uint32_t nvals = 0;       // prefetched value of each pin's next event (pins < 16)
     uint64_t nvals_hi = 0;
     uint32_t has_wave = 0, clock_mask = 0, at_lo = 0, last_rise = 0;
+    // the cell's periodic clock pin (bit pkbit, at most one), not merged:
+    // its edges alternate between phase pA (to 1 - pv0) and pB (back to pv0)
+    // of each cycle; edge j of the tile lies in tile cycle j / 2; bit 30 of
+    // pBv: the edge at time_max is absent
+    uint32_t pkbit = 0, pA = 0, pBv = 0;
     auto get_v = [&](uint32_t s_lo, uint64_t s_hi, int i) -> int {
       return i < 16 ? static_cast<int>((s_lo >> (2 * i)) & 3) : static_cast<int>((s_hi >> (2 * (i - 16))) & 3);
     };
@@ -400,7 +475,17 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       if (i < n_pin) {
         const int32_t net = __ldg(p.pin_net + p0 + i);
         const uint8_t pf = __ldg(p.pin_flags + p0 + i);
-        if (pf & 4) clock_mask |= 1u << i;
+        if (pf & 4) {
+          clock_mask |= 1u << i;
+          if (runs_on && !pkbit && net >= 0 && bins.off >= 0) {
+            const int2 pc = __ldg(p.pclk + net);
+            if (pc.x >= 0) {
+              pkbit = 1u << i;
+              pA = static_cast<uint32_t>(pc.x);
+              pBv = static_cast<uint32_t>(pc.y);
+            }
+          }
+        }
         int v = pf & 3;
         if (net >= 0) {
           const int64_t a = __ldg(p.net_off + net), e = __ldg(p.net_off + net + 1);
@@ -448,6 +533,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
             }
           }
         }
+        if ((pkbit >> i) & 1) {  // its edges are accounted by runs, not merged
+          nt[i] = kRelInf;
+          rem[i] = 0;
+          need &= ~(1u << i);
+        }
         set_v(state, state_hi, i, v);
         if (v == 1) ones |= 1u << i;
       }
@@ -462,6 +552,88 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     double acc_int = 0, acc_gint = 0, acc_sw = 0, acc_gsw = 0, acc_leak = 0;
     uint32_t n_ev = 0, n_gl = 0, n_half = 0, n_rel = 0;
     float leak_cur = leak_of(ones);
+    // clock runs: between two changes of the cell's other pins the clock's
+    // edges see one state s; the edges to 1 - pv0 (A) and back (B) carry the
+    // internal energies eA, eB, and the leakage is lA at pv0, lB at 1 - pv0
+    const int pk = pkbit ? __ffs(pkbit) - 1 : -1;
+    const uint32_t pB = pBv & 0x3fffffffu;
+    const bool p_end_tmax = (pBv >> 30) & 1u;
+    const int pv0 = static_cast<int>(pBv >> 31);
+    uint32_t pj = 0, pjend = 0;  // next edge of the tile not yet accounted; end of the tile's edges
+    // one edge j, with the contributions the merge would give it
+    auto pclk_edge = [&](uint32_t j, float eA, float eB, float lA, float lB) {
+      const int64_t ce = bins.c_lo + (j >> 1);
+      const int64_t te = T0 + static_cast<int64_t>(static_cast<int32_t>((j >> 1) * tpc32) - static_cast<int32_t>(off0) +
+                                                   static_cast<int32_t>((j & 1) ? pB : pA));
+      const bool ea = !(j & 1);
+      const float en = ea ? eA : eB;
+      acc_int += en;
+      add_bin(p, bins, kInt, ce, to_fx(en, p.fx_dyn));
+      const double dl = ea ? static_cast<double>(lB) - static_cast<double>(lA)
+                           : static_cast<double>(lA) - static_cast<double>(lB);
+      if (dl != 0.0) {
+        const double cur_s = static_cast<double>(te) * p.ts;
+        const double end_s = fmin(static_cast<double>(ce + 1) * P, p.tmax_s);
+        add_bin(p, bins, kLeakPart, ce, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin(p, bins, kLeakLevel, ce + 1, to_fx(dl * P, p.fx_leak));
+        acc_leak += dl * static_cast<double>(p.tmax - te);
+      }
+      if (COUNTS) {
+        ++n_ev;
+        n_half += 2;
+        add_cnt(p, bins, 0, ce);
+      }
+    };
+    // edges [pj, jhi) under state s (the other pins' bits): a lone edge at
+    // either end, whole cycles as run-differences (per cycle the sums of the
+    // two edges' contributions; the leakage level steps cancel in a cycle)
+    auto pclk_close = [&](uint32_t jhi, uint32_t s) {
+      if (jhi <= pj) return;
+      uint32_t a = pj, b = jhi;
+      pj = jhi;
+      const uint32_t oA = s | (pv0 ? pkbit : 0u);
+      const uint32_t oB = s | (pv0 ? 0u : pkbit);
+      const float eA = in_energy(pk, oA, pv0 == 0);
+      const float eB = in_energy(pk, oB, pv0 != 0);
+      const float lA = leak_of(oA), lB = leak_of(oB);
+      if (a & 1) pclk_edge(a++, eA, eB, lA, lB);
+      if (b > a && (b & 1)) pclk_edge(--b, eA, eB, lA, lB);
+      if (b > a) {
+        const uint32_t k1 = a >> 1, k2 = b >> 1;
+        const double n = static_cast<double>(k2 - k1);
+        const double dl = static_cast<double>(lB) - static_cast<double>(lA);
+        const unsigned long long e2 = to_fx(eA, p.fx_dyn) + to_fx(eB, p.fx_dyn);
+        const unsigned long long l2 = to_fx(dl * (static_cast<double>(pB - pA) * p.ts), p.fx_leak);
+        acc_int += n * (static_cast<double>(eA) + static_cast<double>(eB));
+        acc_leak += n * dl * static_cast<double>(pB - pA);
+        unsigned long long* run = bins.s + bins.off;
+        if (e2) {
+          atomicAdd(run + kIntRun * ct + k1, e2);
+          if (k2 < ct) atomicAdd(run + kIntRun * ct + k2, 0ull - e2);
+        }
+        if (l2) {
+          atomicAdd(run + kLeakRun * ct + k1, l2);
+          if (k2 < ct) atomicAdd(run + kLeakRun * ct + k2, 0ull - l2);
+        }
+        if (COUNTS) {
+          n_ev += 2 * (k2 - k1);
+          n_half += 4 * (k2 - k1);
+          for (uint32_t k = k1; k < k2; ++k) atomicAdd(bins.sc + k, 2u);
+        }
+      }
+    };
+    if (pkbit) {
+      // first edge at or after max(0, r_exist); the last before span (or
+      // before time_max when the edge there is absent)
+      const uint32_t ph0 = off0 + static_cast<uint32_t>(max(0, r_exist));
+      pj = ph0 <= pA ? 0u : (ph0 <= pB ? 1u : 2u);
+      const int64_t r_end = p_end_tmax ? min(static_cast<int64_t>(span), p.tmax - T0) : static_cast<int64_t>(span);
+      if (r_end > 0) {
+        const uint32_t ce = udiv32(static_cast<uint32_t>(r_end - 1) + off0, tpc32, p.tpc_magic);
+        const int32_t he = static_cast<int32_t>(static_cast<uint32_t>(r_end - 1) + off0 - ce * tpc32);
+        pjend = 2 * ce + (he >= static_cast<int32_t>(pA) ? 1u : 0u) + (he >= static_cast<int32_t>(pB) ? 1u : 0u);
+      }
+    }
     if (owns_initial) {
       acc_leak += static_cast<double>(leak_cur) * static_cast<double>(p.tmax);
       add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak_cur) * P, p.fx_leak));
@@ -496,6 +668,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       const int64_t cyc = bins.c_lo + cq;
       const int32_t cs_rel = static_cast<int32_t>(cq * tpc32) - static_cast<int32_t>(off0);  // cycle start - T0
       const int32_t ce_rel = cs_rel + static_cast<int32_t>(tpc32);
+      // periodic clock: its value before cur (edges strictly before cur)
+      const int32_t ph = static_cast<int32_t>(cur) - cs_rel;
+      const bool p_hi_pre = ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB);
+      if (pkbit) ones = (ones & ~pkbit) | ((p_hi_pre ? pv0 == 0 : pv0 != 0) ? pkbit : 0u);
 
       // advance every pin with an event at cur
       const uint32_t old_state = state;
@@ -545,6 +721,22 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       }
 
       if (RING) do_refills(static_cast<int64_t>(cur));
+
+      // periodic clock: its edges up to cur belong to the run of the old
+      // state; the leakage step of the other pins is taken at the clock's
+      // value after cur
+      if (pkbit) {
+        // an absent edge at time_max does not switch the clock
+        const bool hi = (p_end_tmax && cur_abs >= p.tmax)
+                            ? p_hi_pre
+                            : (ph >= static_cast<int32_t>(pA) && ph < static_cast<int32_t>(pB));
+        const uint32_t cb = (hi ? pv0 == 0 : pv0 != 0) ? pkbit : 0u;
+        ones = (ones & ~pkbit) | cb;
+        leak_cur = leak_of((old_ones & ~pkbit) | cb);
+        if ((ones ^ old_ones) & ~pkbit)
+          pclk_close(min(pjend, 2 * cq + (ph >= static_cast<int32_t>(pA) ? 1u : 0u) + (ph >= static_cast<int32_t>(pB) ? 1u : 0u)),
+                     old_ones & ~pkbit);
+      }
 
       // leakage: level change at cur
       if (DRIFT && pend) apply_pending(cur_abs);
@@ -608,20 +800,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 
         float energy = 0.0f;
         if (i < n_in) {
-          if (FAST) {
-            const int16_t eo = fast_tab[fo + i * n_state + old_ones];
-            if (eo >= 0) energy = blk[eo + (rise ? 0 : 1)];
-          } else {
-            const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + i);
-            const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + i + 1);
-            for (int32_t k = s_begin; k < s_end; ++k) {
-              const DevSlot sl = p.slots[k];
-              if (when_holds(p.cubes, sl.cube_off, sl.n_cube, old_ones)) {
-                energy = blk[sl.e_off + (rise ? 0 : 1)];
-                break;
-              }
-            }
-          }
+          energy = in_energy(i, old_ones, rise);
         } else {
           const int o = i - n_in;
           float best = p.min_diff0;
@@ -633,9 +812,23 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
           for (int q = 0; q < (MAXP < 2 ? 1 : MAXP - 1); ++q) {
             if (q >= n_in) break;
             if (!((has_wave >> q) & 1)) continue;
-            const int32_t tr = lt[q];
+            int32_t tr = lt[q];
+            bool fr = (last_rise >> q) & 1;
+            if ((pkbit >> q) & 1) {
+              // the periodic clock's last edge strictly before cur, when it
+              // lies in the window (else the last event before the window)
+              const uint32_t jb = 2 * cq + (ph > static_cast<int32_t>(pA) ? 1u : 0u) + (ph > static_cast<int32_t>(pB) ? 1u : 0u);
+              if (jb >= 1) {
+                const uint32_t jl = jb - 1;
+                const int32_t te = static_cast<int32_t>((jl >> 1) * tpc32) - static_cast<int32_t>(off0) +
+                                   static_cast<int32_t>((jl & 1) ? pB : pA);
+                if (te >= r_exist) {
+                  tr = te;
+                  fr = (jl & 1) ? (pv0 != 0) : (pv0 == 0);
+                }
+              }
+            }
             if (tr < cs_rel || tr >= ce_rel) continue;  // the related pin's edge lies in this cycle
-            const bool fr = (last_rise >> q) & 1;
             const float dl = dlp[q * 4 + (fr ? 0 : 2)];
             if (isnan(dl)) continue;
             const double trs = __dmul_rn(static_cast<double>(T0 + tr), p.ts);
@@ -706,6 +899,8 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       at_lo &= ~trig;
     }
 
+    if (pkbit) pclk_close(pjend, ones & ~pkbit);
+
     if (DRIFT && pend) {
       // end of the pending segment: the cell's next event, or time_max
       int64_t q = p.tmax;
@@ -732,6 +927,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   }
 
   __syncthreads();
+  // clock runs: run-differences -> per-cycle sums
+  if (runs_on) {
+    for (int set = 0; set < nset; ++set) {
+      block_inclusive_scan(smem + static_cast<int64_t>(set) * nslot * ct + kIntRun * ct, ct, s_wsum);
+      block_inclusive_scan(smem + static_cast<int64_t>(set) * nslot * ct + kLeakRun * ct, ct, s_wsum);
+    }
+  }
   // flush the tile's per-cycle bins
   const int64_t stride = p.n_period + 1;
   for (int64_t k = threadIdx.x; k < ct; k += blockDim.x) {
@@ -739,8 +941,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     const int64_t cc = c < p.n_period ? c : p.n_period;
 #pragma unroll
     for (int q = 0; q < kNumCycAcc; ++q) {
-      const unsigned long long x0 = smem[q * ct + k];
-      const unsigned long long x1 = nset == 2 ? smem[(kNumCycAcc + q) * ct + k] : 0ull;
+      unsigned long long x0 = smem[q * ct + k];
+      unsigned long long x1 = nset == 2 ? smem[(nslot + q) * ct + k] : 0ull;
+      if (runs_on && (q == kInt || q == kLeakPart)) {
+        const int r = q == kInt ? kIntRun : kLeakRun;
+        x0 += smem[r * ct + k];
+        if (nset == 2) x1 += smem[(nslot + r) * ct + k];
+      }
       if (x0 + x1) atomicAdd(p.cyc_acc + q * stride + cc, x0 + x1);
       if (p.cyc_acc_g) {
         if (x0) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g_first) * kNumCycAcc + q) * stride + cc, x0);
@@ -756,10 +963,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 }
 
 // One window of one design: block (x, y) walks gate block x over tile y.
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
   extern __shared__ unsigned long long smem[];
-  walk_block<MAXP, COUNTS, FAST, DRIFT>(p, blockIdx.x, blockIdx.y, smem);
+  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 // Persistent walk over the windows of many designs: each block takes work
@@ -767,7 +974,7 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const 
 // z: tile) from a queue in descending order of estimated work until it is
 // empty. *n_items and the queue head *counter live in device memory, so a
 // captured launch can be replayed with new items.
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
     power_walk_batch_kernel(const KParams* __restrict__ params, const int4* __restrict__ items,
                             const int* __restrict__ n_items, int* __restrict__ counter) {
@@ -785,7 +992,7 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sp);
     for (int k = threadIdx.x; k < static_cast<int>(sizeof(KParams) / 8); k += blockDim.x) dst[k] = src[k];
     __syncthreads();
-    walk_block<MAXP, COUNTS, FAST, DRIFT>(sp, w.y, w.z, smem);
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS>(sp, w.y, w.z, smem);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
@@ -846,6 +1053,83 @@ __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ p
   }
 }
 
+// ---- periodic clock patterns ----
+
+// First index in [lo, hi) whose event time is >= x.
+__device__ __forceinline__ int64_t lower_bound_time(const int64_t* __restrict__ t, int64_t lo, int64_t hi, int64_t x) {
+  while (lo < hi) {
+    const int64_t m = lo + ((hi - lo) >> 1);
+    if (ev_time(t, m) < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// out[nets[w]] = the window's periodic pattern of net nets[w], one warp per
+// net: its events in [TL, TH) = [max(t_lo, 1), min(t_hi, tmax + 1)) are edge
+// k0, k0 + 1, ... of the sequence whose edge k lies at (k / 2) * tpc + (k odd
+// ? pb : pa) with value (k odd ? v0 : 1 - v0), no edge of the sequence in
+// [TL, TH) is missing but one at exactly time_max (a trace that ends on a
+// clock edge it does not list; flagged in bit 30 of y), and the last event
+// before TL holds the value before edge k0. Otherwise x = -1 and the walk
+// takes the net's events one by one.
+__global__ void pclk_kernel(const KParams pv, const KParams* __restrict__ pd, const int32_t* __restrict__ nets,
+                            int32_t n, int2* __restrict__ out) {
+  const KParams& p = pd ? *pd : pv;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t w = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; w < n; w += warps) {
+    const int32_t net = nets[w];
+    if (net < 0 || net >= p.n_net) continue;
+    const int64_t lo = p.net_off[net], hi = p.net_off[net + 1];
+    const int64_t tpc = p.tpc;
+    bool ok = lo >= 0 && hi >= lo && hi <= p.n_event && tpc >= 2 && tpc < (int64_t(1) << 30);
+    const int64_t TL = max(p.t_lo, static_cast<int64_t>(1)), TH = min(p.t_hi, p.tmax + 1);
+    int64_t l = lo, u = lo;
+    if (ok) {
+      l = lower_bound_time(p.ev_t, lo, hi, TL);
+      u = lower_bound_time(p.ev_t, l, hi, TH);
+      // two edges to read the phases from, a value before them, and no
+      // event past time_max inside the window (the walk reports those)
+      ok = u - l >= 2 && l > lo && (u == hi || ev_time(p.ev_t, u) >= p.t_hi);
+    }
+    int64_t pa = 0, pb = 0, k0 = 0;
+    int v0 = 0;
+    bool end_tmax = false;
+    if (ok) {
+      const int64_t t0 = ev_time(p.ev_t, l), t1 = ev_time(p.ev_t, l + 1);
+      const int64_t c0 = t0 / tpc, c1 = t1 / tpc;
+      const int64_t f0 = t0 - c0 * tpc, f1 = t1 - c1 * tpc;
+      const int va = ev_value(p.ev_v, l);
+      if (c1 == c0) {
+        pa = f0; pb = f1; k0 = 2 * c0; v0 = 1 - va;
+      } else if (c1 == c0 + 1 && f1 < f0) {
+        pa = f1; pb = f0; k0 = 2 * c0 + 1; v0 = va;
+      } else {
+        ok = false;
+      }
+      ok = ok && (va == 0 || va == 1) && ev_value(p.ev_v, l - 1) == ((k0 & 1) ? 1 - v0 : v0);
+      const int64_t km = k0 - 1, kn = k0 + (u - l);
+      const int64_t tn = (kn >> 1) * tpc + ((kn & 1) ? pb : pa);
+      end_tmax = tn == p.tmax && p.tmax < TH;
+      ok = ok && (km >> 1) * tpc + ((km & 1) ? pb : pa) < TL && (tn >= TH || end_tmax);
+    }
+    if (ok) {
+      bool good = true;
+      for (int64_t j = lane; j < u - l; j += 32) {
+        const int64_t k = k0 + j;
+        good = good && ev_time(p.ev_t, l + j) == (k >> 1) * tpc + ((k & 1) ? pb : pa) &&
+               ev_value(p.ev_v, l + j) == ((k & 1) ? v0 : 1 - v0);
+      }
+      ok = __all_sync(0xffffffffu, good);
+    }
+    if (lane == 0)
+      out[net] = ok ? make_int2(static_cast<int>(pa),
+                                static_cast<int>(static_cast<uint32_t>(pb) | (end_tmax ? (1u << 30) : 0u) |
+                                                 (static_cast<uint32_t>(v0) << 31)))
+                    : make_int2(-1, 0);
+  }
+}
+
 // ---- walk order by work ----
 
 __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
@@ -857,7 +1141,11 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
   long long w = 0;
   for (int32_t q = a; q < e; ++q) {
     const int32_t net = p.pin_net[q];
-    if (net >= 0) w += p.net_off[net + 1] - p.net_off[net];
+    if (net < 0) continue;
+    // a periodic clock pin of a cell in the first bucket (the fast walk)
+    // costs the walk per change of the other pins only
+    if (p.pclk && k < b1 && (p.pin_flags[q] & 4) && p.pclk[net].x >= 0) continue;
+    w += p.net_off[net + 1] - p.net_off[net];
   }
   const unsigned long long bucket = k >= b2 ? 2ull : (k >= b1 ? 1ull : 0ull);
   const unsigned long long cap = (1ull << 40) - 1;
@@ -877,6 +1165,14 @@ cudaError_t launch_glitch_pw(const KParams& p, const KParams* d_p, float* out, c
   const int64_t threads = static_cast<int64_t>(p.n_net) * 32;
   const int blocks = static_cast<int>(std::min<int64_t>((threads + 255) / 256, 148 * 32));
   glitch_pw_kernel<<<blocks, 256, 0, stream>>>(p, d_p, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pclk(const KParams& p, const KParams* d_p, const int32_t* nets, int32_t n, int2* out,
+                        cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(n) * 32 + 255) / 256, 148 * 8));
+  pclk_kernel<<<blocks, 256, 0, stream>>>(p, d_p, nets, n, out);
   return cudaGetLastError();
 }
 
@@ -1014,7 +1310,7 @@ __global__ void finalize_cycles(const KParams p, const unsigned long long* __res
   }
 }
 
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
 cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   const int32_t n = p.order_end - p.order_begin;
   if (n <= 0) return cudaSuccess;
@@ -1022,8 +1318,8 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
   const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads,
                                             (FAST && WALK_USE_RING) ? MAXP : 0, tabs,
-                                            p.cell_cgroup ? 2 : 1);
-  auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT>;
+                                            p.cell_cgroup ? 2 : 1, RUNS && p.pclk != nullptr);
+  auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT, RUNS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -1032,10 +1328,10 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
 cudaError_t launch_batch_t(const KParams* d_params, const int4* d_items, const int* d_n_items, int* d_counter,
                            int grid, int threads, size_t smem, cudaStream_t stream) {
-  auto kern = power_walk_batch_kernel<MAXP, COUNTS, FAST, DRIFT>;
+  auto kern = power_walk_batch_kernel<MAXP, COUNTS, FAST, DRIFT, RUNS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   kern<<<grid, threads, smem, stream>>>(d_params, d_items, d_n_items, d_counter);
@@ -1047,35 +1343,33 @@ cudaError_t launch_batch_t(const KParams* d_params, const int4* d_items, const i
 static_assert(sizeof(KParams) % 8 == 0, "KParams is copied to shared memory in 8-byte words");
 
 cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items, const int* d_n_items,
-                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, int threads,
-                                    size_t smem, cudaStream_t stream) {
+                                    int* d_counter, int grid, int max_pins, bool counts, bool drift, bool runs,
+                                    int threads, size_t smem, cudaStream_t stream) {
+#define GTPB_BATCH(MP, C, F, D, R) \
+  launch_batch_t<MP, C, F, D, R>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
   if (max_pins <= kFastPins) {
-    if (drift) return counts ? launch_batch_t<kFastPins, true, true, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                             : launch_batch_t<kFastPins, false, true, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
-    return counts ? launch_batch_t<kFastPins, true, true, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                  : launch_batch_t<kFastPins, false, true, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+    if (drift) return counts ? GTPB_BATCH(kFastPins, true, true, true, false) : GTPB_BATCH(kFastPins, false, true, true, false);
+    if (runs) return counts ? GTPB_BATCH(kFastPins, true, true, false, true) : GTPB_BATCH(kFastPins, false, true, false, true);
+    return counts ? GTPB_BATCH(kFastPins, true, true, false, false) : GTPB_BATCH(kFastPins, false, true, false, false);
   }
   if (max_pins <= 8) {
-    if (drift) return counts ? launch_batch_t<8, true, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                             : launch_batch_t<8, false, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
-    return counts ? launch_batch_t<8, true, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                  : launch_batch_t<8, false, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+    if (drift) return counts ? GTPB_BATCH(8, true, false, true, false) : GTPB_BATCH(8, false, false, true, false);
+    return counts ? GTPB_BATCH(8, true, false, false, false) : GTPB_BATCH(8, false, false, false, false);
   }
-  if (drift) return counts ? launch_batch_t<kMaxPins, true, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                           : launch_batch_t<kMaxPins, false, false, true>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
-  return counts ? launch_batch_t<kMaxPins, true, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream)
-                : launch_batch_t<kMaxPins, false, false, false>(d_params, d_items, d_n_items, d_counter, grid, threads, smem, stream);
+  if (drift) return counts ? GTPB_BATCH(kMaxPins, true, false, true, false) : GTPB_BATCH(kMaxPins, false, false, true, false);
+  return counts ? GTPB_BATCH(kMaxPins, true, false, false, false) : GTPB_BATCH(kMaxPins, false, false, false, false);
+#undef GTPB_BATCH
 }
 
 int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem) {
   int nb = 0;
   cudaError_t e;
   if (max_pins <= kFastPins)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kFastPins, false, true, true>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kFastPins, false, true, true, false>, threads, smem);
   else if (max_pins <= 8)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<8, false, false, true>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<8, false, false, true, false>, threads, smem);
   else
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kMaxPins, false, false, true>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kMaxPins, false, false, true, false>, threads, smem);
   (void)counts;
   (void)drift;
   return e == cudaSuccess && nb > 0 ? nb : 1;
@@ -1088,12 +1382,13 @@ size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int thr
                     : 0;
   if (fast && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
   return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, (fast && WALK_USE_RING) ? kFastPins : 0, tabs,
-                               p.cell_cgroup ? 2 : 1);
+                               p.cell_cgroup ? 2 : 1, fast && !p.drift && p.pclk != nullptr);
 }
 
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
-                             size_t tab_bytes, int bin_sets) {
-  return static_cast<size_t>(cycles_per_tile) * (bin_sets * kNumCycAcc * 8 + (counts ? 8 : 0)) +
+                             size_t tab_bytes, int bin_sets, bool clock_runs) {
+  const int slots = clock_runs ? kNumBinSlotsRun : kNumCycAcc;
+  return static_cast<size_t>(cycles_per_tile) * (bin_sets * slots * 8 + (counts ? 8 : 0)) +
          static_cast<size_t>(ring_pins) * kRing * threads * 4 + tab_bytes;
 }
 
@@ -1103,6 +1398,8 @@ cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int t
   if (max_pins <= kFastPins) {
     if (d) return counts ? launch_t<kFastPins, true, true, true>(p, threads, stream)
                          : launch_t<kFastPins, false, true, true>(p, threads, stream);
+    if (p.pclk) return counts ? launch_t<kFastPins, true, true, false, true>(p, threads, stream)
+                              : launch_t<kFastPins, false, true, false, true>(p, threads, stream);
     return counts ? launch_t<kFastPins, true, true, false>(p, threads, stream)
                   : launch_t<kFastPins, false, true, false>(p, threads, stream);
   }

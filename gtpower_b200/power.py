@@ -85,7 +85,8 @@ class B200Power:
 
     def __init__(self, design: Design, *, collect_counts: bool = False, device: int = -1,
                  cycles_per_tile: int = 0, threads_per_block: int = 0, gates_per_block: int = 0,
-                 max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None):
+                 max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None,
+                 clock_runs: bool = True):
         self.design = design
         L = _abi.lib()
         cfg = _abi.gtp_config()
@@ -98,6 +99,8 @@ class B200Power:
         cfg.max_n_pin_for_leakage_power = max_n_pin_for_leakage_power
         if sort_by_work is not None:
             cfg.sort_by_work = 1 if sort_by_work else 0
+        # periodic clock pins walked as runs of whole cycles (False: edge by edge)
+        cfg.clock_runs = 1 if clock_runs else -1
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()
@@ -169,6 +172,13 @@ class B200Power:
         assert g.shape == (self.design.n_cell,)
         _abi.check(_abi.lib().gtp_set_cycle_groups(self.ctx, g.ctypes.data_as(C.c_void_p), int(n_group)),
                    self.ctx)
+
+    def clock_run_nets(self) -> tuple[int, int]:
+        """(nets read by clock pins, those the last window walked as runs of
+        whole cycles because their events were exactly periodic)."""
+        n_clk, n_per = C.c_int32(0), C.c_int32(0)
+        _abi.check(_abi.lib().gtp_clock_run_nets(self.ctx, C.byref(n_clk), C.byref(n_per)), self.ctx)
+        return int(n_clk.value), int(n_per.value)
 
     def fetch_cycle_groups(self) -> np.ndarray:
         """[n_group, 5, n_period] float32: the cycle5 rows of each group."""

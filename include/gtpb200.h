@@ -205,7 +205,11 @@ typedef struct gtp_config {
   int32_t sort_by_work;              /* 1 = per window, walk cells in order of their
                                         event count so a warp's cells carry similar
                                         work (default 1) */
-  int32_t reserved32;
+  int32_t clock_runs;                /* clock pins whose net is exactly periodic in a
+                                        window (one rise and one fall per cycle at
+                                        fixed phases) are walked as runs of whole
+                                        cycles between the cell's other events:
+                                        0 or 1 = on (default), -1 = edge by edge */
   int64_t reserved[3];
 } gtp_config;
 
@@ -289,6 +293,13 @@ gtp_status  gtp_set_cycle_groups(gtp_ctx* ctx, const int32_t* cell_group, int32_
 int32_t     gtp_n_cycle_groups(const gtp_ctx* ctx);
 /* cycle5_groups [n_group][5][n_period]: per group, the rows of cycle5. */
 gtp_status  gtp_fetch_cycle_groups(gtp_ctx* ctx, float* cycle5_groups);
+
+/* Clock runs (gtp_config.clock_runs); no counterpart in the reference, a
+ * diagnostic of this engine. *n_clock_nets = nets read by clock pins,
+ * *n_periodic = those whose events in the last pushed window were exactly
+ * periodic, so that the walk took their clock pins as runs of whole cycles
+ * (0 when clock runs are off). Waits for the context's stream. */
+gtp_status  gtp_clock_run_nets(gtp_ctx* ctx, int32_t* n_clock_nets, int32_t* n_periodic);
 
 /* Allocation-free evaluation. No counterpart in the reference.
  *

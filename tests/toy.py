@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from gtpower_b200.design import CellLibrary, Design, Events, GROUP_COMBINATIONAL
+from gtpower_b200.design import CellLibrary, Design, Events, GROUP_COMBINATIONAL, GROUP_SEQUENTIAL
 
 
 def table1(axis, values):
@@ -171,4 +171,116 @@ def random_design(rng: np.random.Generator, n_cell: int, n_net: int, time_max: i
     d.pin_slew_fall = rng.uniform(5e-11, 5e-10, d.n_pin).astype(np.float32)
     inf_mask = rng.random(d.n_pin) < 0.02
     d.pin_slew_rise[inf_mask] = np.inf
+    return d, events(n_net, per)
+
+
+def dff_cell(name="DFF", clk_first=False):
+    """Flip-flop D, CLK -> Q (CLK first with clk_first). The clock pin's
+    energies depend on D and Q (one fall energy negative), D's on the clock
+    value, Q's tables are related to CLK and to D, and all 8 leakage states
+    differ (the clock value included)."""
+    i_d, i_c = (1, 0) if clk_first else (0, 1)
+    bd, bc, bq = 1 << i_d, 1 << i_c, 1 << 2
+    pins = [None, None, {"name": "Q", "direction": "output", "capacitance": 0.0, "clock": False}]
+    pins[i_d] = {"name": "D", "direction": "input", "capacitance": 1e-15, "clock": False}
+    pins[i_c] = {"name": "CLK", "direction": "input", "capacitance": 2e-15, "clock": True}
+    ip = [
+        {"pin": i_c, "related_pin": -1, "when": [[bd | bq, bd]], "rise": const(6e-15), "fall": const(2e-15)},
+        {"pin": i_c, "related_pin": -1, "when": [[bd, bd]], "rise": const(5e-15), "fall": const(3e-15)},
+        {"pin": i_c, "related_pin": -1, "when": [[0, 0]], "rise": table1([0.0, 1e-9], [1e-15, 4e-15]),
+         "fall": const(-1e-15)},
+        {"pin": i_d, "related_pin": -1, "when": [[bc, bc]], "rise": const(2e-15), "fall": const(2.5e-15)},
+        {"pin": i_d, "related_pin": -1, "when": [[bc, 0]], "rise": const(1e-15), "fall": const(1.5e-15)},
+        {"pin": 2, "related_pin": i_c, "when": [[0, 0]], "rise": const(20e-15), "fall": const(25e-15)},
+        {"pin": 2, "related_pin": i_d, "when": [[0, 0]], "rise": const(8e-15), "fall": const(9e-15)},
+    ]
+    leaks = [{"when": [[7, s]], "power": (1 + s) * 1e-9 + (3e-9 if s & bc else 0.0)} for s in range(8)]
+    return {"name": name, "n_in": 2, "pins": pins, "internal_powers": ip, "leakage_powers": leaks,
+            "cell_leakage_power": 2e-9, "is_sequential": True, "is_pad": False, "is_macro": False,
+            "timing": [], "functions": {}}
+
+
+def clock_wave(tpc: int, time_max: int, pa: int, pb: int, v0: int, *, initial=True,
+               gap=None) -> list[tuple[int, int]]:
+    """Periodic clock: edge to 1 - v0 at phase pa and back to v0 at phase pb
+    of every cycle, from an initial value at tick 0 (none: the clock is X
+    until its first edge); gap = (c0, c1) drops the edges of cycles c0..c1-1
+    (a stopped clock)."""
+    ev = []
+    if initial:
+        ev.append((0, v0 if pa > 0 else 1 - v0))
+    for c in range(time_max // tpc + 1):
+        if gap is not None and gap[0] <= c < gap[1]:
+            continue
+        for ph, v in ((pa, 1 - v0), (pb, v0)):
+            t = c * tpc + ph
+            if 0 < t <= time_max:
+                ev.append((t, v))
+    return ev
+
+
+def clocked_design(rng: np.random.Generator, n_dff: int, n_comb: int, n_data: int, tpc: int,
+                   n_cycle: int, clocks: list[dict], tail: int = 0):
+    """Random flip-flop design on periodic clocks. clocks: dicts with pa, pb,
+    v0 and optional initial / gap (clock_wave). Flip-flop outputs change a
+    few ticks after their clock's edges; data events fall on random ticks, a
+    third of them on a clock edge; some values are X or Z. An inverter on
+    each clock net (not a clock pin) reads the clock as data."""
+    cells = [dff_cell(), dff_cell("DFFC", clk_first=True), inv_cell(), nand_cell()]
+    time_max = n_cycle * tpc - tail
+    n_clk = len(clocks)
+    waves = [clock_wave(tpc, time_max, c["pa"], c["pb"], c["v0"], initial=c.get("initial", True),
+                        gap=c.get("gap")) for c in clocks]
+    n_q = n_dff
+    d0 = n_clk                       # data nets
+    q0 = n_clk + n_data              # flip-flop outputs
+    x0 = q0 + n_q                    # combinational outputs
+    n_net = x0 + n_comb + n_clk
+    per = {k: waves[k] for k in range(n_clk)}
+    edge_t = [np.asarray([t for t, _ in w if t > 0], np.int64) for w in waves]
+
+    def data_events(k):
+        n = int(rng.integers(2, 4 * n_cycle))
+        ts = rng.integers(1, time_max + 1, size=n)
+        snap = rng.random(n) < 0.33
+        allt = np.concatenate(edge_t) if edge_t else np.zeros(0, np.int64)
+        if allt.size:
+            ts[snap] = rng.choice(allt, size=int(snap.sum()))
+        ts = np.unique(ts)
+        vals = rng.choice([0, 1, 2, 3], size=ts.size, p=[0.45, 0.45, 0.06, 0.04])
+        return [(0, int(rng.integers(0, 2)))] + list(zip(ts.tolist(), vals.tolist()))
+
+    for k in range(n_data):
+        per[d0 + k] = data_events(k)
+    inst = []
+    for i in range(n_dff):
+        ck = int(rng.integers(0, n_clk))
+        d = d0 + int(rng.integers(0, n_data))
+        q = q0 + i
+        t = int(rng.integers(0, 2))
+        inst.append((t, [ck, d, q] if t == 1 else [d, ck, q]))
+        # Q follows some edges of its clock after 1..40 ticks
+        et = edge_t[ck]
+        qs = np.unique(np.minimum(et[rng.random(et.size) < 0.3] + int(rng.integers(1, 41)), time_max))
+        per[q] = [(0, 0)] + [(int(t_), int(v)) for t_, v in zip(qs.tolist(), (np.arange(qs.size) + 1) % 2)]
+    for j in range(n_comb):
+        a = int(rng.integers(0, q0 + n_q))
+        b = int(rng.integers(0, q0 + n_q))
+        inst.append((3, [a, b, x0 + j]))
+        per[x0 + j] = data_events(j)
+    for k in range(n_clk):
+        inst.append((2, [k, x0 + n_comb + k]))
+    n_pin = sum(len(p) for _, p in inst)
+    clock_pins = []
+    off = 0
+    for t, pins in inst:
+        if t in (0, 1):
+            clock_pins.append(off + (1 if t == 0 else 0))
+        off += len(pins)
+    d = build(cells, inst, n_net, period=tpc * 1e-12, time_max=time_max,
+              arcs=lambda i, o, q, fr, to: float(rng.uniform(1e-12, 3e-11)) if rng.random() < 0.9 else np.nan,
+              clock_pins=clock_pins,
+              groups=[GROUP_SEQUENTIAL if t in (0, 1) else GROUP_COMBINATIONAL for t, _ in inst])
+    d.pin_slew_rise = rng.uniform(5e-11, 5e-10, d.n_pin).astype(np.float32)
+    d.pin_slew_fall = rng.uniform(5e-11, 5e-10, d.n_pin).astype(np.float32)
     return d, events(n_net, per)
