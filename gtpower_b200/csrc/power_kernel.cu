@@ -47,6 +47,9 @@ constexpr int32_t kFarBefore = INT32_MIN / 2;
 #ifndef WALK_RING
 #define WALK_RING 8
 #endif
+#ifndef WALK_KEY_CLASS
+#define WALK_KEY_CLASS 1    // cells with a periodic clock pin sort apart from the others
+#endif
 #ifndef WALK_USE_RING
 #define WALK_USE_RING 0
 #endif
@@ -555,11 +558,18 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     // clock runs: between two changes of the cell's other pins the clock's
     // edges see one state s; the edges to 1 - pv0 (A) and back (B) carry the
     // internal energies eA, eB, and the leakage is lA at pv0, lB at 1 - pv0
-    const int pk = pkbit ? __ffs(pkbit) - 1 : -1;
     const uint32_t pB = pBv & 0x3fffffffu;
-    const bool p_end_tmax = (pBv >> 30) & 1u;
     const int pv0 = static_cast<int>(pBv >> 31);
-    uint32_t pj = 0, pjend = 0;  // next edge of the tile not yet accounted; end of the tile's edges
+    uint32_t pj = 0;  // next edge of the tile not yet accounted
+    // end of the tile's edges: those before span, or before time_max when the
+    // edge there is absent
+    auto pclk_jend = [&]() -> uint32_t {
+      const int64_t r_end = ((pBv >> 30) & 1u) ? min(static_cast<int64_t>(span), p.tmax - T0) : static_cast<int64_t>(span);
+      if (r_end <= 0) return 0u;
+      const uint32_t ce = udiv32(static_cast<uint32_t>(r_end - 1) + off0, tpc32, p.tpc_magic);
+      const int32_t he = static_cast<int32_t>(static_cast<uint32_t>(r_end - 1) + off0 - ce * tpc32);
+      return 2 * ce + (he >= static_cast<int32_t>(pA) ? 1u : 0u) + (he >= static_cast<int32_t>(pB) ? 1u : 0u);
+    };
     // one edge j, with the contributions the merge would give it
     auto pclk_edge = [&](uint32_t j, float eA, float eB, float lA, float lB) {
       const int64_t ce = bins.c_lo + (j >> 1);
@@ -591,6 +601,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       if (jhi <= pj) return;
       uint32_t a = pj, b = jhi;
       pj = jhi;
+      const int pk = __ffs(pkbit) - 1;
       const uint32_t oA = s | (pv0 ? pkbit : 0u);
       const uint32_t oB = s | (pv0 ? 0u : pkbit);
       const float eA = in_energy(pk, oA, pv0 == 0);
@@ -623,16 +634,9 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       }
     };
     if (pkbit) {
-      // first edge at or after max(0, r_exist); the last before span (or
-      // before time_max when the edge there is absent)
+      // first edge at or after max(0, r_exist)
       const uint32_t ph0 = off0 + static_cast<uint32_t>(max(0, r_exist));
       pj = ph0 <= pA ? 0u : (ph0 <= pB ? 1u : 2u);
-      const int64_t r_end = p_end_tmax ? min(static_cast<int64_t>(span), p.tmax - T0) : static_cast<int64_t>(span);
-      if (r_end > 0) {
-        const uint32_t ce = udiv32(static_cast<uint32_t>(r_end - 1) + off0, tpc32, p.tpc_magic);
-        const int32_t he = static_cast<int32_t>(static_cast<uint32_t>(r_end - 1) + off0 - ce * tpc32);
-        pjend = 2 * ce + (he >= static_cast<int32_t>(pA) ? 1u : 0u) + (he >= static_cast<int32_t>(pB) ? 1u : 0u);
-      }
     }
     if (owns_initial) {
       acc_leak += static_cast<double>(leak_cur) * static_cast<double>(p.tmax);
@@ -670,8 +674,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       const int32_t ce_rel = cs_rel + static_cast<int32_t>(tpc32);
       // periodic clock: its value before cur (edges strictly before cur)
       const int32_t ph = static_cast<int32_t>(cur) - cs_rel;
-      const bool p_hi_pre = ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB);
-      if (pkbit) ones = (ones & ~pkbit) | ((p_hi_pre ? pv0 == 0 : pv0 != 0) ? pkbit : 0u);
+      if (pkbit) {
+        const bool hi = ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB);
+        ones = (ones & ~pkbit) | ((hi ? pv0 == 0 : pv0 != 0) ? pkbit : 0u);
+      }
 
       // advance every pin with an event at cur
       const uint32_t old_state = state;
@@ -726,16 +732,18 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       // state; the leakage step of the other pins is taken at the clock's
       // value after cur
       if (pkbit) {
-        // an absent edge at time_max does not switch the clock
-        const bool hi = (p_end_tmax && cur_abs >= p.tmax)
-                            ? p_hi_pre
-                            : (ph >= static_cast<int32_t>(pA) && ph < static_cast<int32_t>(pB));
+        // edges at or before cur, but an absent edge at time_max
+        const bool at_end = ((pBv >> 30) & 1u) && cur_abs >= p.tmax;
+        const bool hi = at_end ? (ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB))
+                               : (ph >= static_cast<int32_t>(pA) && ph < static_cast<int32_t>(pB));
         const uint32_t cb = (hi ? pv0 == 0 : pv0 != 0) ? pkbit : 0u;
         ones = (ones & ~pkbit) | cb;
         leak_cur = leak_of((old_ones & ~pkbit) | cb);
-        if ((ones ^ old_ones) & ~pkbit)
-          pclk_close(min(pjend, 2 * cq + (ph >= static_cast<int32_t>(pA) ? 1u : 0u) + (ph >= static_cast<int32_t>(pB) ? 1u : 0u)),
-                     old_ones & ~pkbit);
+        if ((ones ^ old_ones) & ~pkbit) {
+          uint32_t jhi = 2 * cq + (ph >= static_cast<int32_t>(pA) ? 1u : 0u) + (ph >= static_cast<int32_t>(pB) ? 1u : 0u);
+          if (at_end) jhi = min(jhi, pclk_jend());
+          pclk_close(jhi, old_ones & ~pkbit);
+        }
       }
 
       // leakage: level change at cur
@@ -899,7 +907,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       at_lo &= ~trig;
     }
 
-    if (pkbit) pclk_close(pjend, ones & ~pkbit);
+    if (pkbit) pclk_close(pclk_jend(), ones & ~pkbit);
 
     if (DRIFT && pend) {
       // end of the pending segment: the cell's next event, or time_max
@@ -1139,23 +1147,30 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
   const int32_t cell = base_order[k];
   const int32_t a = p.cell_pin_off[cell], e = p.cell_pin_off[cell + 1];
   long long w = 0;
+  bool pclk_cell = false;
   for (int32_t q = a; q < e; ++q) {
     const int32_t net = p.pin_net[q];
     if (net < 0) continue;
     // a periodic clock pin of a cell in the first bucket (the fast walk)
     // costs the walk per change of the other pins only
-    if (p.pclk && k < b1 && (p.pin_flags[q] & 4) && p.pclk[net].x >= 0) continue;
+    if (p.pclk && k < b1 && (p.pin_flags[q] & 4) && p.pclk[net].x >= 0) {
+      pclk_cell = true;
+      continue;
+    }
     w += p.net_off[net + 1] - p.net_off[net];
   }
   const unsigned long long bucket = k >= b2 ? 2ull : (k >= b1 ? 1ull : 0ull);
-  const unsigned long long cap = (1ull << 40) - 1;
+  const unsigned long long cap = (1ull << 39) - 1;
   const unsigned long long wc = w < 0 ? 0ull : (static_cast<unsigned long long>(w) > cap ? cap : static_cast<unsigned long long>(w));
-  // bits [0,40): inverted work; then the bucket, or with per-cycle groups
-  // the cell group in [40,58) and the bucket in [58,60)
+  // bits [0,39): inverted work; bit 39: the cell has a periodic clock pin
+  // (its lanes take the clock-run branches, so such cells share warps); then
+  // the bucket, or with per-cycle groups the cell group in [40,58) and the
+  // bucket in [58,60)
+  const unsigned long long cls = (WALK_KEY_CLASS && pclk_cell) ? (1ull << 39) : 0ull;
   if (p.cell_cgroup)
-    keys[k] = (bucket << 58) | (static_cast<unsigned long long>(p.cell_cgroup[cell]) << 40) | (cap - wc);
+    keys[k] = (bucket << 58) | (static_cast<unsigned long long>(p.cell_cgroup[cell]) << 40) | cls | (cap - wc);
   else
-    keys[k] = (bucket << 40) | (cap - wc);
+    keys[k] = (bucket << 40) | cls | (cap - wc);
 }
 
 }  // namespace
