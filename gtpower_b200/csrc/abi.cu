@@ -192,7 +192,8 @@ KParams make_params(gtp_ctx* c) {
 // buffers, tables, and 1 KB for the walk's static shared memory) stays
 // within 227 KB.
 int64_t max_cycles_per_tile(int threads, int bin_sets, bool clock_runs = false) {
-  const int64_t budget = 226 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4));
+  const int64_t budget = 226 * 1024 - static_cast<int64_t>(power_walk_smem_bytes(0, false, threads, kFastPins, 16384 + threads * 65 * 4)) -
+                         static_cast<int64_t>(clock_runs ? walk_runs_acc_bytes(threads) : 0);
   const int slots = clock_runs ? kNumBinSlotsRun : kNumCycAcc;
   return std::max<int64_t>(1, std::min<int64_t>(3072, budget / (bin_sets * slots * 8 + 8)));
 }
@@ -1044,6 +1045,9 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     key.push_back(reinterpret_cast<uint64_t>(kwin[i].glitch_pw));
     key.push_back(static_cast<uint64_t>(first_entry[i]));
   }
+  // clock-run launches keep the threads' per-cell sums ahead of each item's bins
+  for (int g = 0; g < kBatchGroups; ++g)
+    if (runs_g[g]) smem_g[g] += walk_runs_acc_bytes(b->threads);
   int grid_g[kBatchGroups];
   for (int g = 0; g < kBatchGroups; ++g) {
     grid_g[g] = 0;

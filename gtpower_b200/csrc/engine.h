@@ -220,6 +220,10 @@ int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets = 1, bool clock_runs = false);
 
+// Shared memory the clock-run walk (RUNS kernels) adds to the bytes above:
+// the threads' per-cell sums.
+size_t walk_runs_acc_bytes(int threads);
+
 // Fills the pattern table p.pclk (`out`) for the n nets in `nets` over the
 // window p describes: a net is periodic when its events in [max(t_lo, 1),
 // min(t_hi, tmax + 1)) are exactly one edge at phase x and one at phase y of

@@ -298,6 +298,14 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   // each set carries the two clock-run slots
   static_assert(!RUNS || (FAST && !DRIFT), "clock runs need the fast walk without drift");
   const bool runs_on = RUNS && p.pclk != nullptr;
+  // RUNS: each thread's per-cell FP64 sums live in shared memory (slot q of
+  // thread t at s_acc[t * 5 + q]: an odd stride of 8-byte words, free of bank
+  // conflicts), ahead of the bins, to leave the registers to the walk
+  double* s_acc = nullptr;
+  if (RUNS) {
+    s_acc = reinterpret_cast<double*>(smem) + threadIdx.x * kNumCellAcc;
+    smem += kNumCellAcc * blockDim.x;
+  }
   const int nslot = runs_on ? kNumBinSlotsRun : kNumCycAcc;
   __shared__ unsigned long long s_wsum[32];
   Bins bins;
@@ -552,7 +560,16 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     auto leak_of = [&](uint32_t o) -> float {
       return leak_off >= 0 ? leak_pool[leak_off + o] : leak_const;
     };
-    double acc_int = 0, acc_gint = 0, acc_sw = 0, acc_gsw = 0, acc_leak = 0;
+    // per-cell sums: internal, glitch internal, switching, glitch switching,
+    // leakage (registers, or shared slots with RUNS)
+    double acc_r[kNumCellAcc] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (RUNS)
+#pragma unroll
+      for (int q = 0; q < kNumCellAcc; ++q) s_acc[q] = 0.0;
+    auto acc_add = [&](int q, double x) {
+      if (RUNS) s_acc[q] += x;
+      else acc_r[q] += x;
+    };
     uint32_t n_ev = 0, n_gl = 0, n_half = 0, n_rel = 0;
     float leak_cur = leak_of(ones);
     // clock runs: between two changes of the cell's other pins the clock's
@@ -577,7 +594,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
                                                    static_cast<int32_t>((j & 1) ? pB : pA));
       const bool ea = !(j & 1);
       const float en = ea ? eA : eB;
-      acc_int += en;
+      acc_add(0, en);
       add_bin(p, bins, kInt, ce, to_fx(en, p.fx_dyn));
       const double dl = ea ? static_cast<double>(lB) - static_cast<double>(lA)
                            : static_cast<double>(lA) - static_cast<double>(lB);
@@ -586,7 +603,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         const double end_s = fmin(static_cast<double>(ce + 1) * P, p.tmax_s);
         add_bin(p, bins, kLeakPart, ce, to_fx(dl * (end_s - cur_s), p.fx_leak));
         add_bin(p, bins, kLeakLevel, ce + 1, to_fx(dl * P, p.fx_leak));
-        acc_leak += dl * static_cast<double>(p.tmax - te);
+        acc_add(4, dl * static_cast<double>(p.tmax - te));
       }
       if (COUNTS) {
         ++n_ev;
@@ -615,8 +632,8 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         const double dl = static_cast<double>(lB) - static_cast<double>(lA);
         const unsigned long long e2 = to_fx(eA, p.fx_dyn) + to_fx(eB, p.fx_dyn);
         const unsigned long long l2 = to_fx(dl * (static_cast<double>(pB - pA) * p.ts), p.fx_leak);
-        acc_int += n * (static_cast<double>(eA) + static_cast<double>(eB));
-        acc_leak += n * dl * static_cast<double>(pB - pA);
+        acc_add(0, n * (static_cast<double>(eA) + static_cast<double>(eB)));
+        acc_add(4, n * dl * static_cast<double>(pB - pA));
         unsigned long long* run = bins.s + bins.off;
         if (e2) {
           atomicAdd(run + kIntRun * ct + k1, e2);
@@ -639,7 +656,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       pj = ph0 <= pA ? 0u : (ph0 <= pB ? 1u : 2u);
     }
     if (owns_initial) {
-      acc_leak += static_cast<double>(leak_cur) * static_cast<double>(p.tmax);
+      acc_add(4, static_cast<double>(leak_cur) * static_cast<double>(p.tmax));
       add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak_cur) * P, p.fx_leak));
     }
     // drift path: a segment whose seconds cycle precedes its tick cycle
@@ -756,7 +773,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         const double end_s = fmin(static_cast<double>(s + 1) * P, p.tmax_s);
         add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
         add_bin(p, bins, kLeakLevel, s + 1, to_fx(dl * P, p.fx_leak));
-        acc_leak += dl * static_cast<double>(p.tmax - cur_abs);
+        acc_add(4, dl * static_cast<double>(p.tmax - cur_abs));
       }
       if (DRIFT && s != cyc) {
         if (s == cyc + 1) {
@@ -870,10 +887,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
             const float esw = __fmul_rn(nr2 == 2 ? 1.0f : 0.5f, __ldg(p.pin_swe + p0 + i));
             if (g > 0.0f) {
               const float x = __fmul_rn(g, esw);
-              acc_gsw += x;
+              acc_add(3, x);
               add_bin(p, bins, kGSw, cyc, to_fx(x, p.fx_dyn));
             } else {
-              acc_sw += esw;
+              acc_add(2, esw);
               add_bin(p, bins, kSw, cyc, to_fx(esw, p.fx_dyn));
             }
           }
@@ -881,11 +898,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         energy = __fmul_rn(energy, tog2 == 2 ? 1.0f : (tog2 == 1 ? 0.5f : 0.0f));
         if (g > 0.0f) {
           const float x = __fmul_rn(g, energy);
-          acc_gint += x;
+          acc_add(1, x);
           add_bin(p, bins, kGInt, cyc, to_fx(x, p.fx_dyn));
           if (COUNTS) { ++n_gl; add_cnt(p, bins, 1, cyc); }
         } else {
-          acc_int += energy;
+          acc_add(0, energy);
           add_bin(p, bins, kInt, cyc, to_fx(energy, p.fx_dyn));
         }
         if (COUNTS) {
@@ -921,11 +938,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 
     // flush the cell's sums for this tile
     const int64_t nc = p.n_cell;
-    if (acc_int != 0) atomicAdd(p.cell_acc + 0 * nc + cell, acc_int);
-    if (acc_gint != 0) atomicAdd(p.cell_acc + 1 * nc + cell, acc_gint);
-    if (acc_sw != 0) atomicAdd(p.cell_acc + 2 * nc + cell, acc_sw);
-    if (acc_gsw != 0) atomicAdd(p.cell_acc + 3 * nc + cell, acc_gsw);
-    if (acc_leak != 0) atomicAdd(p.cell_acc + 4 * nc + cell, acc_leak);
+#pragma unroll
+    for (int q = 0; q < kNumCellAcc; ++q) {
+      const double a = RUNS ? s_acc[q] : acc_r[q];
+      if (a != 0) atomicAdd(p.cell_acc + q * nc + cell, a);
+    }
     if (COUNTS) {
       if (n_ev) atomicAdd(p.cnt_cell + 0 * nc + cell, n_ev);
       if (n_gl) atomicAdd(p.cnt_cell + 1 * nc + cell, n_gl);
@@ -1333,7 +1350,8 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
   const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads,
                                             (FAST && WALK_USE_RING) ? MAXP : 0, tabs,
-                                            p.cell_cgroup ? 2 : 1, RUNS && p.pclk != nullptr);
+                                            p.cell_cgroup ? 2 : 1, RUNS && p.pclk != nullptr) +
+                      (RUNS ? walk_runs_acc_bytes(threads) : 0);
   auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT, RUNS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -1399,6 +1417,8 @@ size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int thr
   return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, (fast && WALK_USE_RING) ? kFastPins : 0, tabs,
                                p.cell_cgroup ? 2 : 1, fast && !p.drift && p.pclk != nullptr);
 }
+
+size_t walk_runs_acc_bytes(int threads) { return static_cast<size_t>(kNumCellAcc) * 8 * threads; }
 
 size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, int ring_pins,
                              size_t tab_bytes, int bin_sets, bool clock_runs) {
