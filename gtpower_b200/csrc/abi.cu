@@ -176,6 +176,7 @@ KParams make_params(gtp_ctx* c) {
   k.min_diff0 = static_cast<float>(static_cast<double>(P.tmax) * P.ts);
   k.fx_dyn = c->fx_dyn;
   k.fx_leak = c->fx_leak;
+  k.fx_dyn_f = (c->fx_dyn >= 1.0 && c->fx_dyn <= std::ldexp(1.0, 126)) ? static_cast<float>(c->fx_dyn) : 0.0f;
   k.cell_acc = c->d_cell_acc;
   k.cyc_acc = c->d_cyc_acc;
   k.cnt_cell = c->d_cnt_cell;

@@ -169,6 +169,9 @@ struct KParams {
   // fixed point scales (J -> int64)
   double fx_dyn;
   double fx_leak;
+  float fx_dyn_f;                   // fx_dyn as a float when it is a power of two >= 1 within
+                                    // float range (float energies then scale exactly in FP32), else 0
+  int32_t fx_pad;
   // accumulators
   double* cell_acc;                 // [5][n_cell]
   unsigned long long* cyc_acc;      // [6][n_period+1]

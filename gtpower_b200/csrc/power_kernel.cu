@@ -110,6 +110,14 @@ __device__ __forceinline__ unsigned long long to_fx(double x, double s) {
   return static_cast<unsigned long long>(__double2ll_rn(x * s));
 }
 
+// to_fx of a float energy at the scale fx_dyn: with fs = fx_dyn as a float
+// (a power of two >= 1, and |e| * fs <= 2^32), e * fs is exact in FP32 and
+// rounds to the same integer as the FP64 product.
+__device__ __forceinline__ unsigned long long to_fx_f(float e, float fs, double s) {
+  if (fs != 0.0f) return static_cast<unsigned long long>(__float2ll_rn(__fmul_rn(e, fs)));
+  return to_fx(static_cast<double>(e), s);
+}
+
 // Reads element i of a register array without dynamic indexing.
 template <int N, typename T>
 __device__ __forceinline__ T sel(const T (&a)[N], int i) {
@@ -121,7 +129,7 @@ __device__ __forceinline__ T sel(const T (&a)[N], int i) {
 }
 
 struct Bins {
-  unsigned long long* s;   // [sets][6][ct] fixed-point energies
+  unsigned long long* s;   // [sets][slots][ct] fixed-point energies
   uint32_t* sc;            // [2][ct] counts
   int64_t c_lo;            // first cycle of the tile
   int64_t ct;              // cycles in the tile
@@ -149,6 +157,16 @@ __device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, 
     if (p.cyc_acc_g)
       atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(b.g) * kNumCycAcc + q) * (p.n_period + 1) + cc, x);
   }
+}
+
+// add_bin for cycle c_lo + k of the tile (k >= 0): the shared bin when k < ct
+__device__ __forceinline__ void add_bin_k(const KParams& p, const Bins& b, int q, uint32_t k,
+                                          unsigned long long x) {
+  if (x == 0ull) return;
+  if (k < static_cast<uint32_t>(b.ct) && b.off >= 0)
+    atomicAdd(b.s + b.off + static_cast<uint32_t>(q) * static_cast<uint32_t>(b.ct) + k, x);
+  else
+    add_bin(p, b, q, b.c_lo + k, x);
 }
 
 __device__ __forceinline__ void add_cnt(const KParams& p, const Bins& b, int q, int64_t c) {
@@ -595,14 +613,14 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       const bool ea = !(j & 1);
       const float en = ea ? eA : eB;
       acc_add(0, en);
-      add_bin(p, bins, kInt, ce, to_fx(en, p.fx_dyn));
+      add_bin_k(p, bins, kInt, j >> 1, to_fx_f(en, p.fx_dyn_f, p.fx_dyn));
       const double dl = ea ? static_cast<double>(lB) - static_cast<double>(lA)
                            : static_cast<double>(lA) - static_cast<double>(lB);
       if (dl != 0.0) {
         const double cur_s = static_cast<double>(te) * p.ts;
         const double end_s = fmin(static_cast<double>(ce + 1) * P, p.tmax_s);
-        add_bin(p, bins, kLeakPart, ce, to_fx(dl * (end_s - cur_s), p.fx_leak));
-        add_bin(p, bins, kLeakLevel, ce + 1, to_fx(dl * P, p.fx_leak));
+        add_bin_k(p, bins, kLeakPart, j >> 1, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin_k(p, bins, kLeakLevel, (j >> 1) + 1, to_fx(dl * P, p.fx_leak));
         acc_add(4, dl * static_cast<double>(p.tmax - te));
       }
       if (COUNTS) {
@@ -630,7 +648,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         const uint32_t k1 = a >> 1, k2 = b >> 1;
         const double n = static_cast<double>(k2 - k1);
         const double dl = static_cast<double>(lB) - static_cast<double>(lA);
-        const unsigned long long e2 = to_fx(eA, p.fx_dyn) + to_fx(eB, p.fx_dyn);
+        const unsigned long long e2 = to_fx_f(eA, p.fx_dyn_f, p.fx_dyn) + to_fx_f(eB, p.fx_dyn_f, p.fx_dyn);
         const unsigned long long l2 = to_fx(dl * (static_cast<double>(pB - pA) * p.ts), p.fx_leak);
         acc_add(0, n * (static_cast<double>(eA) + static_cast<double>(eB)));
         acc_add(4, n * dl * static_cast<double>(pB - pA));
@@ -771,8 +789,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         const double dl = static_cast<double>(leak_new) - static_cast<double>(leak_cur);
         const double cur_s = static_cast<double>(cur_abs) * p.ts;
         const double end_s = fmin(static_cast<double>(s + 1) * P, p.tmax_s);
-        add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
-        add_bin(p, bins, kLeakLevel, s + 1, to_fx(dl * P, p.fx_leak));
+        if (DRIFT) {
+          add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
+          add_bin(p, bins, kLeakLevel, s + 1, to_fx(dl * P, p.fx_leak));
+        } else {  // s is the tick cycle c_lo + cq
+          add_bin_k(p, bins, kLeakPart, cq, to_fx(dl * (end_s - cur_s), p.fx_leak));
+          add_bin_k(p, bins, kLeakLevel, cq + 1, to_fx(dl * P, p.fx_leak));
+        }
         acc_add(4, dl * static_cast<double>(p.tmax - cur_abs));
       }
       if (DRIFT && s != cyc) {
@@ -888,10 +911,10 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
             if (g > 0.0f) {
               const float x = __fmul_rn(g, esw);
               acc_add(3, x);
-              add_bin(p, bins, kGSw, cyc, to_fx(x, p.fx_dyn));
+              add_bin_k(p, bins, kGSw, cq, to_fx_f(x, p.fx_dyn_f, p.fx_dyn));
             } else {
               acc_add(2, esw);
-              add_bin(p, bins, kSw, cyc, to_fx(esw, p.fx_dyn));
+              add_bin_k(p, bins, kSw, cq, to_fx_f(esw, p.fx_dyn_f, p.fx_dyn));
             }
           }
         }
@@ -899,11 +922,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         if (g > 0.0f) {
           const float x = __fmul_rn(g, energy);
           acc_add(1, x);
-          add_bin(p, bins, kGInt, cyc, to_fx(x, p.fx_dyn));
+          add_bin_k(p, bins, kGInt, cq, to_fx_f(x, p.fx_dyn_f, p.fx_dyn));
           if (COUNTS) { ++n_gl; add_cnt(p, bins, 1, cyc); }
         } else {
           acc_add(0, energy);
-          add_bin(p, bins, kInt, cyc, to_fx(energy, p.fx_dyn));
+          add_bin_k(p, bins, kInt, cq, to_fx_f(energy, p.fx_dyn_f, p.fx_dyn));
         }
         if (COUNTS) {
           ++n_ev;
