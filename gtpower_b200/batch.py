@@ -155,8 +155,8 @@ class Shape:
                     gates_per_block=self.gates_per_block)
 
 
-DEFAULT_CANDIDATES = (Shape(512, 256, 256), Shape(512, 256, 1024), Shape(256, 256, 256),
-                      Shape(1024, 256, 256), Shape(512, 128, 256), Shape(512, 256, 512))
+DEFAULT_CANDIDATES = (Shape(512, 256, 256), Shape(768, 256, 256), Shape(512, 256, 1024), Shape(256, 256, 256),
+                      Shape(1024, 256, 256), Shape(512, 128, 256))
 
 
 def tune(designs, windows, candidates=DEFAULT_CANDIDATES, repeats: int = 2, log=None):

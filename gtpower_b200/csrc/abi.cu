@@ -232,7 +232,9 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   const int64_t cyc_end = last_tick / P.tpc + 1;
   const int64_t n_cyc = std::max<int64_t>(1, cyc_end - k.cyc0);
   int64_t ct = c->cfg.cycles_per_tile;
-  if (ct <= 0) ct = c->n_cgroup > 0 ? 512 : 1024;  // per-group bins double the tile's shared memory
+  // 768 cycles keep two blocks per SM with the event buffers; per-group bins
+  // double the tile's shared memory
+  if (ct <= 0) ct = c->n_cgroup > 0 ? 512 : 768;
   ct = std::min<int64_t>(ct, n_cyc);
   const int threads_ = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   // bins + event buffers + tables within 227 KB of shared memory; tile span

@@ -45,13 +45,13 @@ constexpr uint32_t kRelInf = 0xFFFFFFFFu;     // no further event
 constexpr uint32_t kRelBeyond = 0xFFFFFFFEu;  // next event at or after the tile end
 constexpr int32_t kFarBefore = INT32_MIN / 2;
 #ifndef WALK_RING
-#define WALK_RING 8
+#define WALK_RING 2
 #endif
 #ifndef WALK_KEY_CLASS
 #define WALK_KEY_CLASS 1    // cells with a periodic clock pin sort apart from the others
 #endif
 #ifndef WALK_USE_RING
-#define WALK_USE_RING 0
+#define WALK_USE_RING 1
 #endif
 #ifndef WALK_STAGE_INST
 #define WALK_STAGE_INST 1
@@ -306,7 +306,7 @@ __device__ __forceinline__ float glitch_ratio(const KParams& p, int64_t e, int64
 // One work item of the walk: the cells order[order_begin + gblk * gates_per_block ...]
 // of one pin bucket over cycle tile `tile` of the window, with the block's
 // dynamic shared memory `smem`. All threads of the block call it together.
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS, bool RING_EV>
 __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile,
                                            unsigned long long* smem) {
   const int64_t ct = p.cycles_per_tile;
@@ -338,7 +338,8 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     for (int64_t k = threadIdx.x; k < 2 * ct; k += blockDim.x) bins.sc[k] = 0u;
   // RING: per-thread event buffers [pin][slot][thread] of times - T0, then
   // the per-type energy-selection and leakage tables when they fit
-  constexpr bool RING = FAST && WALK_USE_RING;
+  static_assert(!RING_EV || FAST, "event buffers are for the fast walk");
+  constexpr bool RING = RING_EV;
   constexpr bool STAGE = FAST && WALK_STAGE_INST;
   uint32_t* ring = reinterpret_cast<uint32_t*>(smem + nset * nslot * ct + (COUNTS ? ct : 0));
   const int nt_blk = blockDim.x;
@@ -1014,7 +1015,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
   extern __shared__ unsigned long long smem[];
-  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS>(p, blockIdx.x, blockIdx.y, smem);
+  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, smem);
 }
 
 // Persistent walk over the windows of many designs: each block takes work
@@ -1040,7 +1041,8 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sp);
     for (int k = threadIdx.x; k < static_cast<int>(sizeof(KParams) / 8); k += blockDim.x) dst[k] = src[k];
     __syncthreads();
-    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS>(sp, w.y, w.z, smem);
+    // no event buffers: the persistent walk keeps its shared memory for occupancy
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, false>(sp, w.y, w.z, smem);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
@@ -1437,7 +1439,7 @@ size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int thr
                     ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16
                     : 0;
   if (fast && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
-  return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, (fast && WALK_USE_RING) ? kFastPins : 0, tabs,
+  return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, 0, tabs,
                                p.cell_cgroup ? 2 : 1, fast && !p.drift && p.pclk != nullptr);
 }
 
