@@ -942,10 +942,6 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     gtp_status st = prepare_window(c, ev.net_off, ev.time, ev.value_packed, ev.net_base, ev.n_event, ev.t_lo,
                                    ev.t_hi, b->stream, &kwin[i], false);
     if (st != GTP_OK) return batch_fail(b, st, "context " + std::to_string(i) + ": " + c->err);
-    // the persistent walk takes clock pins edge by edge: measured on 64
-    // synthetic traces, clock runs made it slower (221 against 177 ms per
-    // wave), the opposite of the one-window walk
-    kwin[i].pclk = nullptr;
     active.push_back(i);
     const KParams& k = kwin[i];
     const Packed& P = c->P;
@@ -1062,7 +1058,8 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     const int bk = g / 2;
     const int per_sm = b->cfg.blocks_per_sm > 0
                            ? b->cfg.blocks_per_sm
-                           : walk_blocks_per_sm(bucket_pins[bk], b->counts, (g & 1) != 0, b->threads, smem_g[g]);
+                           : walk_blocks_per_sm(bucket_pins[bk], b->counts, (g & 1) != 0, runs_g[g], b->threads,
+                                                smem_g[g]);
     grid_g[g] = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(b->sm_count) * per_sm,
                                                    static_cast<int64_t>(groups[g].size())));
     key.push_back(static_cast<uint64_t>(g) << 56 | static_cast<uint64_t>(grid_g[g]) << 24 | smem_g[g]);

@@ -216,7 +216,7 @@ cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items
 // Dynamic shared memory of one walk block for these parameters.
 size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int threads);
 // Resident blocks per SM of the persistent walk at this shape.
-int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem);
+int walk_blocks_per_sm(int max_pins, bool counts, bool drift, bool runs, int threads, size_t smem);
 
 // bin_sets: 1, or 2 when per-cycle accumulators are kept by cell group;
 // clock_runs: the bins carry the two clock-run slots (p.pclk set).

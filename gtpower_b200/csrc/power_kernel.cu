@@ -1419,18 +1419,24 @@ cudaError_t launch_power_walk_batch(const KParams* d_params, const int4* d_items
 #undef GTPB_BATCH
 }
 
-int walk_blocks_per_sm(int max_pins, bool counts, bool drift, int threads, size_t smem) {
-  int nb = 0;
-  cudaError_t e;
-  if (max_pins <= kFastPins)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kFastPins, false, true, true, false>, threads, smem);
-  else if (max_pins <= 8)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<8, false, false, true, false>, threads, smem);
-  else
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, power_walk_batch_kernel<kMaxPins, false, false, true, false>, threads, smem);
-  (void)counts;
-  (void)drift;
-  return e == cudaSuccess && nb > 0 ? nb : 1;
+int walk_blocks_per_sm(int max_pins, bool counts, bool drift, bool runs, int threads, size_t smem) {
+  // the kernel that will be launched, with its dynamic shared-memory limit
+  // raised first: above 48 KB the occupancy query fails without it
+  auto occ = [&](auto kern) -> int {
+    int nb = 0;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem);
+    return e == cudaSuccess && nb > 0 ? nb : 1;
+  };
+#define GTPB_OCC(MP, F, D, R) (counts ? occ(power_walk_batch_kernel<MP, true, F, D, R>) \
+                                      : occ(power_walk_batch_kernel<MP, false, F, D, R>))
+  if (max_pins <= kFastPins) {
+    if (drift) return GTPB_OCC(kFastPins, true, true, false);
+    return runs ? GTPB_OCC(kFastPins, true, false, true) : GTPB_OCC(kFastPins, true, false, false);
+  }
+  if (max_pins <= 8) return drift ? GTPB_OCC(8, false, true, false) : GTPB_OCC(8, false, false, false);
+  return drift ? GTPB_OCC(kMaxPins, false, true, false) : GTPB_OCC(kMaxPins, false, false, false);
+#undef GTPB_OCC
 }
 
 size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int threads) {

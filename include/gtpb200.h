@@ -296,11 +296,10 @@ gtp_status  gtp_fetch_cycle_groups(gtp_ctx* ctx, float* cycle5_groups);
 
 /* Clock runs (gtp_config.clock_runs); no counterpart in the reference, a
  * diagnostic of this engine. *n_clock_nets = nets read by clock pins,
- * *n_periodic = those whose events in the last window pushed through
- * gtp_push_events or gtp_push_events_device were exactly periodic, so that
- * the walk took their clock pins as runs of whole cycles (0 when clock runs
- * are off; batched pushes, gtp_batch_push_device, walk every clock edge).
- * Waits for the context's stream. */
+ * *n_periodic = those whose events in the context's last pushed window
+ * (single or batched) were exactly periodic, so that the walk took their
+ * clock pins as runs of whole cycles (0 when clock runs are off). Waits for
+ * the context's stream. */
 gtp_status  gtp_clock_run_nets(gtp_ctx* ctx, int32_t* n_clock_nets, int32_t* n_periodic);
 
 /* Allocation-free evaluation. No counterpart in the reference.
