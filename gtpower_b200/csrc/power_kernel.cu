@@ -53,6 +53,9 @@ constexpr int32_t kFarBefore = INT32_MIN / 2;
 #ifndef WALK_USE_RING
 #define WALK_USE_RING 1
 #endif
+#ifndef WALK_BATCH_RING
+#define WALK_BATCH_RING 1   // event buffers in the persistent batched walk too
+#endif
 #ifndef WALK_STAGE_INST
 #define WALK_STAGE_INST 1
 #endif
@@ -1041,8 +1044,7 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sp);
     for (int k = threadIdx.x; k < static_cast<int>(sizeof(KParams) / 8); k += blockDim.x) dst[k] = src[k];
     __syncthreads();
-    // no event buffers: the persistent walk keeps its shared memory for occupancy
-    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, false>(sp, w.y, w.z, smem);
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_BATCH_RING>(sp, w.y, w.z, smem);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
@@ -1445,7 +1447,7 @@ size_t walk_item_smem_bytes(const KParams& p, int max_pins, bool counts, int thr
                     ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16
                     : 0;
   if (fast && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
-  return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, 0, tabs,
+  return power_walk_smem_bytes(p.cycles_per_tile, counts, threads, (fast && WALK_BATCH_RING) ? kFastPins : 0, tabs,
                                p.cell_cgroup ? 2 : 1, fast && !p.drift && p.pclk != nullptr);
 }
 
