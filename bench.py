@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cycles-per-tile", type=int, default=0)
+    ap.add_argument("--e2e-split", default="ramp", choices=["ramp", "even"],
+                    help="e2e windows: 'ramp' grows them 1.5x each (a short first copy, then each copy "
+                         "hides behind the walk of the window before), 'even' cuts equal windows")
     ap.add_argument("--e2e-windows", type=int, default=4,
                     help="the e2e leg pushes the trace from pinned host memory as this many windows "
                          "(with their context), so that each window's copy overlaps the previous walk")
@@ -615,11 +618,24 @@ def main():
     e2e_wins = []
     h2d = 0
     if args.e2e_windows > 1:
-        st = _synth.Stream(trace, (args.cycles + args.e2e_windows - 1) // args.e2e_windows)
-        while True:
-            w = st.next(n_event + 4 * design.n_net)
-            if w is None:
-                break
+        if args.e2e_split == "ramp":
+            from gtpower_b200 import windows as _windows
+            tpc = design.ticks_per_cycle
+            sizes = 1.5 ** np.arange(args.e2e_windows)
+            cuts = np.concatenate([[0], np.round(np.cumsum(sizes) / sizes.sum() * args.cycles)]).astype(np.int64)
+            cuts = np.unique(cuts)
+            wins_src = [_windows.make_window(ev, tpc, int(cuts[k]) * tpc,
+                                             int(cuts[k + 1]) * tpc if k + 2 < len(cuts) else np.iinfo(np.int64).max)
+                        for k in range(len(cuts) - 1)]
+        else:
+            st = _synth.Stream(trace, (args.cycles + args.e2e_windows - 1) // args.e2e_windows)
+            wins_src = []
+            while True:
+                w = st.next(n_event + 4 * design.n_net)
+                if w is None:
+                    break
+                wins_src.append(w)
+        for w in wins_src:
             pt = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
                   for a in (w.net_off, w.time, w.packed.view(np.int32), w.net_base)]
             e2e_wins.append((pt, Events(pt[0].numpy(), pt[1].numpy(), pt[2].numpy().view(np.uint32),
@@ -734,7 +750,7 @@ def main():
                        "parallelism": f"weak: {world} independent traces" if world > 1 else "1 GPU"},
             "e2e": {"value": world * n_event / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "windows": len(e2e_wins)},
+                    "windows": len(e2e_wins), "split": args.e2e_split if len(e2e_wins) > 1 else "one window"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
