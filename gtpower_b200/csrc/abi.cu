@@ -163,11 +163,13 @@ KParams make_params(gtp_ctx* c) {
   k.tmax_s = static_cast<double>(P.tmax) * P.ts;
   k.n_net = P.n_net;
   k.tpc = P.tpc;
-  k.inv_tpc = 1.0 / static_cast<double>(P.tpc);
   k.tpc_magic = P.tpc >= 2 && P.tpc < (int64_t(1) << 31)
                     ? static_cast<uint32_t>(((uint64_t(1) << 32) + static_cast<uint64_t>(P.tpc) - 1) /
                                             static_cast<uint64_t>(P.tpc))
                     : 0u;
+  k.tpc_magic64 = P.tpc >= 2 ? static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / static_cast<uint64_t>(P.tpc) +
+                                                     ((static_cast<unsigned __int128>(1) << 64) % static_cast<uint64_t>(P.tpc) != 0))
+                              : 0u;
   k.ts = P.ts;
   k.period_d = P.period_d;
   k.inv_period_d = 1.0 / P.period_d;

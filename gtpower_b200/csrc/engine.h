@@ -152,8 +152,8 @@ struct KParams {
   int32_t n_net;
   // time base
   int64_t tpc;
-  double inv_tpc;
   uint32_t tpc_magic;        // ceil(2^32 / tpc) for tpc >= 2 (32-bit division by tpc), 0 for tpc == 1
+  uint64_t tpc_magic64;      // ceil(2^64 / tpc) for tpc >= 2 (division of a tick by tpc), 0 for tpc == 1
   double ts;
   double period_d;
   double inv_period_d;

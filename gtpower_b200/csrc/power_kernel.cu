@@ -61,13 +61,14 @@ constexpr int32_t kFarBefore = INT32_MIN / 2;
 #endif
 constexpr int kRing = WALK_RING;               // events buffered per pin (RING path)
 
-__device__ __forceinline__ int64_t div_floor_pos(int64_t t, int64_t d, double inv) {
-  // floor(t / d) for 0 <= t < 2^53 via a double reciprocal and one correction
-  int64_t q = static_cast<int64_t>(static_cast<double>(t) * inv);
-  int64_t r = t - q * d;
-  if (r < 0) --q;
-  else if (r >= d) ++q;
-  return q;
+// floor(t / d) for 0 <= t < 2^63 and d >= 2 with magic = ceil(2^64 / d)
+// (0 for d == 1): umulhi(t, magic) is floor(t / d) or one more, since
+// t * (magic - 2^64 / d) / 2^64 < 1/2.
+__device__ __forceinline__ int64_t div_floor_t(int64_t t, int64_t d, uint64_t magic) {
+  if (magic == 0u) return t;
+  uint64_t q = __umul64hi(static_cast<uint64_t>(t), magic);
+  if (q * static_cast<uint64_t>(d) > static_cast<uint64_t>(t)) --q;
+  return static_cast<int64_t>(q);
 }
 
 // floor(n / d) for n < 2^31, d < 2^31 with magic = ceil(2^32 / d) (d >= 2):
@@ -265,7 +266,7 @@ __device__ float glitch_pw(const KParams& p, int64_t e, int64_t lo, int64_t hi, 
       pflag = false;
     } else {
       const int64_t tp = ev_time(p.ev_t, e - 1);
-      const int64_t pc = div_floor_pos(tp, p.tpc, p.inv_tpc);
+      const int64_t pc = div_floor_t(tp, p.tpc, p.tpc_magic64);
       const Group gp = period_group(p.ev_t, e - 1, lo, hi, g0, pc * p.tpc, pc * p.tpc + p.tpc);
       const int64_t kp = gp.last - gp.first + 1;   // e-1 is the last of its period
       pflag = kp >= 2 && (kp & 1) == 0;
@@ -278,7 +279,7 @@ __device__ float glitch_pw(const KParams& p, int64_t e, int64_t lo, int64_t hi, 
     if (e + 1 <= gr.last) {
       nflag = (e + 1 - gr.first) < lim;
     } else if (e + 2 < hi) {
-      const int64_t nc = div_floor_pos(tn, p.tpc, p.inv_tpc);
+      const int64_t nc = div_floor_t(tn, p.tpc, p.tpc_magic64);
       nflag = ev_time(p.ev_t, e + 2) < nc * p.tpc + p.tpc;
     } else {
       nflag = false;
@@ -1095,7 +1096,7 @@ __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ p
     const int64_t g0 = base == 0 ? lo : -1;
     for (int64_t e = lo + lane; e < hi; e += 32) {
       const int64_t t = ev_time(p.ev_t, e);
-      const int64_t cyc = div_floor_pos(t, p.tpc, p.inv_tpc);
+      const int64_t cyc = div_floor_t(t, p.tpc, p.tpc_magic64);
       const int64_t cs = cyc * p.tpc;
       // an event alone in its period is never a glitch event
       const bool prev_same = e - 1 >= lo && ev_time(p.ev_t, e - 1) >= cs;
