@@ -243,9 +243,24 @@ __global__ void denorm_kernel(const float* py, int64_t n, int O, int Op, const f
   }
 }
 
+// floor(t / tpc) for 0 < t < 2^63 with magic = ceil(2^64 / tpc) (0 for
+// tpc == 1): umulhi(t, magic) is the quotient or one more.
+__device__ __forceinline__ int64_t cycle_of(int64_t t, int64_t tpc, uint64_t magic) {
+  if (magic == 0u) return t;
+  uint64_t q = __umul64hi(static_cast<uint64_t>(t), magic);
+  if (q * static_cast<uint64_t>(tpc) > static_cast<uint64_t>(t)) --q;
+  return static_cast<int64_t>(q);
+}
+
+uint64_t cycle_magic(int64_t tpc) {
+  if (tpc < 2) return 0u;
+  const unsigned __int128 one = static_cast<unsigned __int128>(1) << 64;
+  return static_cast<uint64_t>(one / static_cast<uint64_t>(tpc) + (one % static_cast<uint64_t>(tpc) != 0));
+}
+
 // One warp per selected net.
 __global__ void toggle_bits_kernel(const int64_t* off, const int64_t* time, const int32_t* sel, int n_sel,
-                                   int64_t tpc, int64_t c_lo, int64_t c_hi, uint16_t* x, int64_t ld) {
+                                   int64_t tpc, uint64_t magic, int64_t c_lo, int64_t c_hi, uint16_t* x, int64_t ld) {
   const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (wid >= n_sel) return;
@@ -254,15 +269,15 @@ __global__ void toggle_bits_kernel(const int64_t* off, const int64_t* time, cons
   for (int64_t i = b + lane; i < e; i += 32) {
     const int64_t t = time[i];
     if (t <= 0) continue;
-    const int64_t c = t / tpc;
+    const int64_t c = cycle_of(t, tpc, magic);
     if (c < c_lo || c >= c_hi) continue;
     x[(c - c_lo) * ld + wid] = 0x3F80;  // 1.0 in BF16
   }
 }
 
 // One warp per net; a cycle counts once however many events it holds.
-__global__ void toggle_stats_kernel(const int64_t* off, const int64_t* time, int n_net, int64_t tpc, int64_t c_lo,
-                                    int64_t c_hi, const float* y, int64_t* count, double* sum_y) {
+__global__ void toggle_stats_kernel(const int64_t* off, const int64_t* time, int n_net, int64_t tpc, uint64_t magic,
+                                    int64_t c_lo, int64_t c_hi, const float* y, int64_t* count, double* sum_y) {
   const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (wid >= n_net) return;
@@ -272,12 +287,12 @@ __global__ void toggle_stats_kernel(const int64_t* off, const int64_t* time, int
   for (int64_t i = b + lane; i < e; i += 32) {
     const int64_t t = time[i];
     if (t <= 0) continue;
-    const int64_t c = t / tpc;
+    const int64_t c = cycle_of(t, tpc, magic);
     if (c < c_lo || c >= c_hi) continue;
     bool first = true;
     if (i > b) {
       const int64_t tp = time[i - 1];
-      first = tp <= 0 || tp / tpc != c;
+      first = tp <= 0 || cycle_of(tp, tpc, magic) != c;
     }
     if (first) {
       ++cnt;
@@ -885,7 +900,7 @@ gtp_status gtp_toggle_bits(const int64_t* d_net_off, const int64_t* d_time, cons
   if (n_sel == 0 || c_hi == c_lo) return GTP_OK;
   const int64_t threads = (int64_t)n_sel * 32;
   toggle_bits_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      d_net_off, d_time, d_sel, n_sel, tpc, c_lo, c_hi, d_x, ld);
+      d_net_off, d_time, d_sel, n_sel, tpc, cycle_magic(tpc), c_lo, c_hi, d_x, ld);
   return cudaGetLastError() == cudaSuccess ? GTP_OK : GTP_ECUDA;
 }
 
@@ -896,7 +911,7 @@ gtp_status gtp_net_toggle_stats(const int64_t* d_net_off, const int64_t* d_time,
   if (n_net == 0 || c_hi == c_lo) return GTP_OK;
   const int64_t threads = (int64_t)n_net * 32;
   toggle_stats_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      d_net_off, d_time, n_net, tpc, c_lo, c_hi, d_y, d_count, d_sum_y);
+      d_net_off, d_time, n_net, tpc, cycle_magic(tpc), c_lo, c_hi, d_y, d_count, d_sum_y);
   return cudaGetLastError() == cudaSuccess ? GTP_OK : GTP_ECUDA;
 }
 
