@@ -94,6 +94,13 @@ class gtp_counts(C.Structure):
                 ("dropped", C.c_int64)]
 
 
+class gtp_bits_window(C.Structure):
+    _fields_ = [("d_net_off", _P), ("d_time", _P), ("c_lo", C.c_int64), ("c_hi", C.c_int64)]
+
+
+BITS_MAX_WINDOWS = 64
+
+
 class gtp_proxy_config(C.Structure):
     _fields_ = [("cuda_device_id", C.c_int32), ("n_in", C.c_int32), ("n_hidden", C.c_int32),
                 ("n_out", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
@@ -119,7 +126,7 @@ EXPORTED = sorted([
     "gtp_proxy_get_stream", "gtp_proxy_set_stream", "gtp_proxy_n_param",
     "gtp_proxy_set_training_data", "gtp_proxy_get_norm", "gtp_proxy_train",
     "gtp_proxy_compute_grads", "gtp_proxy_adam_step", "gtp_proxy_get_params",
-    "gtp_proxy_set_params", "gtp_proxy_get_grads", "gtp_proxy_predict", "gtp_toggle_bits",
+    "gtp_proxy_set_params", "gtp_proxy_get_grads", "gtp_proxy_predict", "gtp_toggle_bits", "gtp_toggle_bits_windows",
     "gtp_net_toggle_stats", "gtp_bf16_gemm",
 ])
 
@@ -216,6 +223,7 @@ def _bind_proxy(L: C.CDLL) -> None:
         "gtp_proxy_get_grads": ([_P, _P], i32),
         "gtp_proxy_predict": ([_P, _P, i64, _P], i32),
         "gtp_toggle_bits": ([_P, _P, _P, i32, i64, i64, i64, _P, i64, _P], i32),
+        "gtp_toggle_bits_windows": ([C.POINTER(gtp_bits_window), i32, _P, i32, i64, i64, _P, i64, _P], i32),
         "gtp_net_toggle_stats": ([_P, _P, i32, i64, i64, i64, _P, _P, _P, _P], i32),
         "gtp_bf16_gemm": ([_P, i64, _P, i64, i64, i64, i64, _P, i32, _P, i64, _P], i32),
     }

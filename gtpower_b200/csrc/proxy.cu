@@ -275,6 +275,64 @@ __global__ void toggle_bits_kernel(const int64_t* off, const int64_t* time, cons
   }
 }
 
+// Dense toggle bits of many windows (gtp_toggle_bits_windows). Block (x, y):
+// nets sel[32x .. 32x + 31] over row chunk y (window w, up to kBitsRows
+// cycles). Masks are built with shared atomics, then written as rows of 32
+// BF16 entries (64 B) per block.
+constexpr int kBitsRows = 2048;
+
+struct BitsLaunch {
+  gtp_bits_window w[GTP_BITS_MAX_WINDOWS];
+  int32_t chunk0[GTP_BITS_MAX_WINDOWS + 1];  // first row chunk of each window
+  int32_t n_win;
+  int32_t pad;
+};
+
+__global__ void __launch_bounds__(256) toggle_bits_windows_kernel(const __grid_constant__ BitsLaunch L,
+                                                                  const int32_t* __restrict__ sel, int n_sel,
+                                                                  int64_t tpc, uint64_t magic, int64_t c_base,
+                                                                  uint16_t* __restrict__ x, int64_t ld) {
+  __shared__ uint32_t bits[kBitsRows];
+  const int ch = blockIdx.y;
+  int wi = 0;
+  while (wi + 1 < L.n_win && L.chunk0[wi + 1] <= ch) ++wi;
+  const gtp_bits_window& win = L.w[wi];
+  const int64_t r_lo = win.c_lo + static_cast<int64_t>(ch - L.chunk0[wi]) * kBitsRows;
+  const int64_t r_hi = min(win.c_hi, r_lo + kBitsRows);
+  const int rows = static_cast<int>(r_hi - r_lo);
+  const int k0 = blockIdx.x * 32;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) bits[r] = 0u;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = warp; j < 32 && k0 + j < n_sel; j += nw) {
+    const int32_t net = __ldg(sel + k0 + j);
+    const int64_t b = __ldg(win.d_net_off + net), e = __ldg(win.d_net_off + net + 1);
+    for (int64_t i = b + lane; i < e; i += 32) {
+      const int64_t t = __ldg(win.d_time + i);
+      if (t <= 0) continue;
+      const int64_t c = cycle_of(t, tpc, magic);
+      if (c >= r_hi) break;  // a lane's later events are later still
+      if (c >= r_lo) atomicOr(bits + (c - r_lo), 1u << j);
+    }
+  }
+  __syncthreads();
+  // lanes 0-15 write one row's 32 entries as 16 pairs, lanes 16-31 the next row's
+  const int half = lane >> 4, q = lane & 15;
+  const int kc = k0 + 2 * q;
+  const bool pairs = (ld & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 3) == 0;
+  for (int r = 2 * warp + half; r < rows; r += 2 * nw) {
+    const uint32_t m = bits[r];
+    uint16_t* row = x + (r_lo + r - c_base) * ld;
+    const uint16_t v0 = ((m >> (2 * q)) & 1u) ? 0x3F80 : 0, v1 = ((m >> (2 * q + 1)) & 1u) ? 0x3F80 : 0;
+    if (kc + 1 < n_sel && pairs) {
+      *reinterpret_cast<uint32_t*>(row + kc) = static_cast<uint32_t>(v0) | (static_cast<uint32_t>(v1) << 16);
+    } else {
+      if (kc < n_sel) row[kc] = v0;
+      if (kc + 1 < n_sel) row[kc + 1] = v1;
+    }
+  }
+}
+
 // One warp per net; a cycle counts once however many events it holds.
 __global__ void toggle_stats_kernel(const int64_t* off, const int64_t* time, int n_net, int64_t tpc, uint64_t magic,
                                     int64_t c_lo, int64_t c_hi, const float* y, int64_t* count, double* sum_y) {
@@ -901,6 +959,33 @@ gtp_status gtp_toggle_bits(const int64_t* d_net_off, const int64_t* d_time, cons
   const int64_t threads = (int64_t)n_sel * 32;
   toggle_bits_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       d_net_off, d_time, d_sel, n_sel, tpc, cycle_magic(tpc), c_lo, c_hi, d_x, ld);
+  return cudaGetLastError() == cudaSuccess ? GTP_OK : GTP_ECUDA;
+}
+
+gtp_status gtp_toggle_bits_windows(const gtp_bits_window* windows, int32_t n_win, const int32_t* d_sel,
+                                   int32_t n_sel, int64_t tpc, int64_t c_base, uint16_t* d_x, int64_t ld,
+                                   void* stream) {
+  if (!windows || n_win < 0 || n_win > GTP_BITS_MAX_WINDOWS || !d_sel || !d_x || n_sel < 0 || tpc <= 0 ||
+      ld < n_sel)
+    return GTP_EINVAL;
+  if (n_sel == 0 || n_win == 0) return GTP_OK;
+  BitsLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  int64_t chunks = 0;
+  for (int i = 0; i < n_win; ++i) {
+    const gtp_bits_window& w = windows[i];
+    if (!w.d_net_off || !w.d_time || w.c_hi < w.c_lo || w.c_lo < c_base) return GTP_EINVAL;
+    L.w[i] = w;
+    L.chunk0[i] = static_cast<int32_t>(chunks);
+    chunks += (w.c_hi - w.c_lo + kBitsRows - 1) / kBitsRows;
+    if (chunks > 65535) return GTP_EOVERFLOW;
+  }
+  L.chunk0[n_win] = static_cast<int32_t>(chunks);
+  L.n_win = n_win;
+  if (chunks == 0) return GTP_OK;
+  dim3 grid(static_cast<unsigned>((n_sel + 31) / 32), static_cast<unsigned>(chunks));
+  toggle_bits_windows_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      L, d_sel, n_sel, tpc, cycle_magic(tpc), c_base, d_x, ld);
   return cudaGetLastError() == cudaSuccess ? GTP_OK : GTP_ECUDA;
 }
 

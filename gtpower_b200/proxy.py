@@ -155,7 +155,9 @@ class PowerProxy:
         n = x.shape[0]
         if out is None:
             out = torch.empty((n, self.n_out), dtype=torch.float32, device=x.device)
-        torch.cuda.current_stream().synchronize()
+        # x and out come from torch's current stream: the proxy's stream waits
+        # for it on the device, with no host stall
+        self.stream.wait_stream(torch.cuda.current_stream())
         self._check(self.L.gtp_proxy_predict(self.h, _ptr(x), n, _ptr(out)))
         if sync:
             self.stream.synchronize()
@@ -174,6 +176,21 @@ def toggle_bits(net_off, time, sel, ticks_per_cycle: int, c_lo: int, c_hi: int, 
                            _ptr(out), out.stride(0), C.c_void_p(stream or 0))
     _abi.check(st)
     return out
+
+
+def toggle_bits_windows(windows, sel, ticks_per_cycle: int, c_base: int, out, stream=None) -> None:
+    """Dense toggle bits of several windows: windows is a list of (net_off,
+    time, c_lo, c_hi) with device event CSRs and disjoint cycle ranges;
+    out[c - c_base, k] = 1.0 or 0.0 for every c in a window's range and
+    k < len(sel). Rows outside the windows are left as they are."""
+    L = _abi.lib()
+    n_sel = int(sel.shape[0])
+    for i in range(0, len(windows), _abi.BITS_MAX_WINDOWS):
+        part = windows[i:i + _abi.BITS_MAX_WINDOWS]
+        arr = (_abi.gtp_bits_window * len(part))(*[
+            _abi.gtp_bits_window(_ptr(no), _ptr(tm), int(lo), int(hi)) for no, tm, lo, hi in part])
+        _abi.check(L.gtp_toggle_bits_windows(arr, len(part), _ptr(sel), n_sel, ticks_per_cycle, c_base,
+                                             _ptr(out), out.stride(0), C.c_void_p(stream or 0)))
 
 
 def net_toggle_stats(net_off, time, n_net: int, ticks_per_cycle: int, c_lo: int, c_hi: int, y,

@@ -207,15 +207,30 @@ def features(windows, sel: np.ndarray, tpc: int, c_lo: int, c_hi: int, out=None)
     torch = _torch()
     k = int(sel.shape[0])
     if out is None:
-        out = torch.zeros((c_hi - c_lo, k), dtype=torch.bfloat16, device="cuda")
-    else:
-        out.zero_()
+        out = torch.empty((c_hi - c_lo, k), dtype=torch.bfloat16, device="cuda")
     d_sel = torch.from_numpy(np.ascontiguousarray(sel, np.int32)).cuda()
+    fill_toggle_bits(out, windows, d_sel, tpc, c_lo, c_hi)
+    return out
+
+
+def fill_toggle_bits(out, windows, d_sel, tpc: int, c_lo: int, c_hi: int, stream=None) -> None:
+    """out[c - c_lo, k] = toggle bit of net d_sel[k] in cycle c for all c in
+    [c_lo, c_hi): the windows' rows written densely in one launch per 64
+    windows, rows of no window zeroed."""
+    spans = []
     for w in windows:
         lo, hi = max(c_lo, w.c_lo), min(c_hi, w.c_hi)
         if lo < hi:
-            px.toggle_bits(w.net_off, w.time, d_sel, tpc, lo, hi, out=out[lo - c_lo:])
-    return out
+            spans.append((w.net_off, w.time, lo, hi))
+    spans.sort(key=lambda s: s[2])
+    done = c_lo
+    for _, _, lo, hi in spans:
+        if lo > done:
+            out[done - c_lo:lo - c_lo].zero_()
+        done = max(done, hi)
+    if done < c_hi:
+        out[done - c_lo:].zero_()
+    px.toggle_bits_windows(spans, d_sel, tpc, c_lo, out, stream=stream)
 
 
 def ridge_fit(X, Y, n_val: int, lams=(1e-3, 1e-2, 1e-1, 1.0, 10.0, 100.0, 1000.0)):
@@ -378,12 +393,7 @@ def run_flow(design, windows: list[DeviceWindow], tpc: int, n_train: int, n_bloc
     with torch.cuda.stream(s):
         for _ in range(2):  # warm-up, then timed
             e0.record(s)
-            X_inf.zero_()
-            for w in windows:
-                lo, hi = max(n_train, w.c_lo), min(n_cycle, w.c_hi)
-                if lo < hi:
-                    px.toggle_bits(w.net_off, w.time, d_sel, tpc, lo, hi, out=X_inf[lo - n_train:],
-                                   stream=s.cuda_stream)
+            fill_toggle_bits(X_inf, windows, d_sel, tpc, n_train, n_cycle, stream=s.cuda_stream)
             e1.record(s)
             pred = net.predict(X_inf, sync=False)
             e2.record(s)

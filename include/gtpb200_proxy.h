@@ -102,6 +102,28 @@ gtp_status  gtp_toggle_bits(const int64_t* d_net_off, const int64_t* d_time, con
                             int32_t n_sel, int64_t ticks_per_cycle, int64_t c_lo, int64_t c_hi,
                             uint16_t* d_x, int64_t ld, void* stream);
 
+/* One window for gtp_toggle_bits_windows: its event CSR (device pointers,
+ * gtp_events layout) and the cycles [c_lo, c_hi) whose rows it fills. */
+typedef struct gtp_bits_window {
+  const int64_t* d_net_off;
+  const int64_t* d_time;
+  int64_t c_lo;
+  int64_t c_hi;
+} gtp_bits_window;
+
+#define GTP_BITS_MAX_WINDOWS 64
+
+/* Dense toggle bits of many windows in one launch: for every window w (host
+ * array, at most GTP_BITS_MAX_WINDOWS, row ranges not overlapping) and every
+ * cycle c in [w.c_lo, w.c_hi), d_x[(c - c_base) * ld + k] = 1.0 (BF16) when
+ * net d_sel[k] has an event with tick > 0 in cycle c, else 0.0, for all
+ * k < n_sel. Rows outside the windows are left unchanged, so d_x needs no
+ * clearing first. Each block builds the toggle masks of 32 nets over up to
+ * 2048 rows in shared memory and writes whole row segments. */
+gtp_status  gtp_toggle_bits_windows(const gtp_bits_window* windows, int32_t n_win, const int32_t* d_sel,
+                                    int32_t n_sel, int64_t ticks_per_cycle, int64_t c_base, uint16_t* d_x,
+                                    int64_t ld, void* stream);
+
 /* For every net n < n_net: d_count[n] += number of cycles in [c_lo, c_hi)
  * in which it toggles, d_sum_y[n] += sum of d_y[c - c_lo] over those cycles.
  * Accumulates, so that windows of one trace can be added up. */

@@ -172,3 +172,33 @@ def test_toggle_bits_and_stats_from_event_csr():
     # windowed: cycles [2, 5) only
     x2 = proxy.toggle_bits(d_off, d_t, sel, tpc, 2, 5).float().cpu().numpy()
     assert np.array_equal(x2, want[2:5])
+
+
+@pytest.mark.parametrize("n_sel", [64, 70])
+def test_dense_toggle_bits_of_windows_match_per_window_bits(n_sel):
+    """gtp_toggle_bits_windows against gtp_toggle_bits window by window: an
+    odd net count (a partial last group of 32, an odd row stride), a window
+    longer than one 2048-row chunk, events outside the windows, rows outside
+    every window left as they were."""
+    torch = _torch()
+    from gtpower_b200 import proxy
+    rng = np.random.default_rng(21 + n_sel)
+    tpc, n_net, n_cyc = 50, 300, 6000
+    sel = torch.from_numpy(rng.choice(n_net, n_sel, replace=False).astype(np.int32)).cuda()
+    windows, ref = [], torch.zeros((n_cyc, n_sel), dtype=torch.bfloat16, device="cuda")
+    cuts = [100, 900, 3700, 3701, 5500]           # rows [0, 100) and [5500, 6000) belong to no window
+    for lo, hi in zip(cuts[:-1], cuts[1:]):
+        counts = rng.integers(0, 60, n_net)
+        off = np.zeros(n_net + 1, np.int64)
+        off[1:] = np.cumsum(counts)
+        t = np.concatenate([np.sort(rng.choice(np.arange((lo - 3) * tpc, (hi + 3) * tpc), c, replace=False))
+                            for c in counts]).astype(np.int64)
+        d_off, d_t = torch.from_numpy(off).cuda(), torch.from_numpy(t).cuda()
+        windows.append((d_off, d_t, lo, hi))
+        proxy.toggle_bits(d_off, d_t, sel, tpc, lo, hi, out=ref[lo:])
+    out = torch.full((n_cyc, n_sel), 7.0, dtype=torch.bfloat16, device="cuda")
+    proxy.toggle_bits_windows(windows, sel, tpc, 0, out)
+    torch.cuda.synchronize()
+    assert torch.equal(out[100:5500], ref[100:5500])
+    assert bool((out[:100] == 7.0).all()) and bool((out[5500:] == 7.0).all())
+    assert float(ref.float().sum()) > 0
