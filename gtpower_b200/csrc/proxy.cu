@@ -276,10 +276,11 @@ __global__ void toggle_bits_kernel(const int64_t* off, const int64_t* time, cons
 }
 
 // Dense toggle bits of many windows (gtp_toggle_bits_windows). Block (x, y):
-// nets sel[32x .. 32x + 31] over row chunk y (window w, up to kBitsRows
-// cycles). Masks are built with shared atomics, then written as rows of 32
-// BF16 entries (64 B) per block.
+// nets sel[64x .. 64x + 63] over row chunk y (window w, up to kBitsRows
+// cycles). 64-bit masks are built with shared atomics, then each warp writes
+// whole rows of 64 BF16 entries (128 B).
 constexpr int kBitsRows = 2048;
+constexpr int kBitsNets = 64;
 
 struct BitsLaunch {
   gtp_bits_window w[GTP_BITS_MAX_WINDOWS];
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(256) toggle_bits_windows_kernel(const __grid_c
                                                                   const int32_t* __restrict__ sel, int n_sel,
                                                                   int64_t tpc, uint64_t magic, int64_t c_base,
                                                                   uint16_t* __restrict__ x, int64_t ld) {
-  __shared__ uint32_t bits[kBitsRows];
+  __shared__ unsigned long long bits[kBitsRows];
   const int ch = blockIdx.y;
   int wi = 0;
   while (wi + 1 < L.n_win && L.chunk0[wi + 1] <= ch) ++wi;
@@ -300,11 +301,11 @@ __global__ void __launch_bounds__(256) toggle_bits_windows_kernel(const __grid_c
   const int64_t r_lo = win.c_lo + static_cast<int64_t>(ch - L.chunk0[wi]) * kBitsRows;
   const int64_t r_hi = min(win.c_hi, r_lo + kBitsRows);
   const int rows = static_cast<int>(r_hi - r_lo);
-  const int k0 = blockIdx.x * 32;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) bits[r] = 0u;
+  const int k0 = blockIdx.x * kBitsNets;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) bits[r] = 0ull;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = warp; j < 32 && k0 + j < n_sel; j += nw) {
+  for (int j = warp; j < kBitsNets && k0 + j < n_sel; j += nw) {
     const int32_t net = __ldg(sel + k0 + j);
     const int64_t b = __ldg(win.d_net_off + net), e = __ldg(win.d_net_off + net + 1);
     for (int64_t i = b + lane; i < e; i += 32) {
@@ -312,18 +313,17 @@ __global__ void __launch_bounds__(256) toggle_bits_windows_kernel(const __grid_c
       if (t <= 0) continue;
       const int64_t c = cycle_of(t, tpc, magic);
       if (c >= r_hi) break;  // a lane's later events are later still
-      if (c >= r_lo) atomicOr(bits + (c - r_lo), 1u << j);
+      if (c >= r_lo) atomicOr(bits + (c - r_lo), 1ull << j);
     }
   }
   __syncthreads();
-  // lanes 0-15 write one row's 32 entries as 16 pairs, lanes 16-31 the next row's
-  const int half = lane >> 4, q = lane & 15;
-  const int kc = k0 + 2 * q;
+  // a warp writes one row: lane l holds entries 2l and 2l + 1
+  const int kc = k0 + 2 * lane;
   const bool pairs = (ld & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 3) == 0;
-  for (int r = 2 * warp + half; r < rows; r += 2 * nw) {
-    const uint32_t m = bits[r];
+  for (int r = warp; r < rows; r += nw) {
+    const unsigned long long m = bits[r];
     uint16_t* row = x + (r_lo + r - c_base) * ld;
-    const uint16_t v0 = ((m >> (2 * q)) & 1u) ? 0x3F80 : 0, v1 = ((m >> (2 * q + 1)) & 1u) ? 0x3F80 : 0;
+    const uint16_t v0 = ((m >> (2 * lane)) & 1ull) ? 0x3F80 : 0, v1 = ((m >> (2 * lane + 1)) & 1ull) ? 0x3F80 : 0;
     if (kc + 1 < n_sel && pairs) {
       *reinterpret_cast<uint32_t*>(row + kc) = static_cast<uint32_t>(v0) | (static_cast<uint32_t>(v1) << 16);
     } else {
@@ -983,7 +983,7 @@ gtp_status gtp_toggle_bits_windows(const gtp_bits_window* windows, int32_t n_win
   L.chunk0[n_win] = static_cast<int32_t>(chunks);
   L.n_win = n_win;
   if (chunks == 0) return GTP_OK;
-  dim3 grid(static_cast<unsigned>((n_sel + 31) / 32), static_cast<unsigned>(chunks));
+  dim3 grid(static_cast<unsigned>((n_sel + kBitsNets - 1) / kBitsNets), static_cast<unsigned>(chunks));
   toggle_bits_windows_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       L, d_sel, n_sel, tpc, cycle_magic(tpc), c_base, d_x, ld);
   return cudaGetLastError() == cudaSuccess ? GTP_OK : GTP_ECUDA;

@@ -118,7 +118,7 @@ typedef struct gtp_bits_window {
  * cycle c in [w.c_lo, w.c_hi), d_x[(c - c_base) * ld + k] = 1.0 (BF16) when
  * net d_sel[k] has an event with tick > 0 in cycle c, else 0.0, for all
  * k < n_sel. Rows outside the windows are left unchanged, so d_x needs no
- * clearing first. Each block builds the toggle masks of 32 nets over up to
+ * clearing first. Each block builds the toggle masks of 64 nets over up to
  * 2048 rows in shared memory and writes whole row segments. */
 gtp_status  gtp_toggle_bits_windows(const gtp_bits_window* windows, int32_t n_win, const int32_t* d_sel,
                                     int32_t n_sel, int64_t ticks_per_cycle, int64_t c_base, uint16_t* d_x,

@@ -174,10 +174,10 @@ def test_toggle_bits_and_stats_from_event_csr():
     assert np.array_equal(x2, want[2:5])
 
 
-@pytest.mark.parametrize("n_sel", [64, 70])
+@pytest.mark.parametrize("n_sel", [64, 70, 130])
 def test_dense_toggle_bits_of_windows_match_per_window_bits(n_sel):
     """gtp_toggle_bits_windows against gtp_toggle_bits window by window: an
-    odd net count (a partial last group of 32, an odd row stride), a window
+    odd net count (a partial last group of 64, an odd row stride), a window
     longer than one 2048-row chunk, events outside the windows, rows outside
     every window left as they were."""
     torch = _torch()
