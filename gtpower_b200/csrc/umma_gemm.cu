@@ -211,6 +211,21 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (nb >= N) break;
         float v[16];
         tc::tmem_ld16(lane_base + static_cast<uint32_t>(c), v);
+        // the chunk's bias: four 16-byte loads when it lies whole and aligned
+        float bv[16];
+        if (mode & EPI_BIAS) {
+          if (nb + 16 <= N && (reinterpret_cast<uintptr_t>(ep.bias + nb) & 15) == 0) {
+            const float4* b4 = reinterpret_cast<const float4*>(ep.bias + nb);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float4 w = __ldg(b4 + q);
+              bv[4 * q + 0] = w.x; bv[4 * q + 1] = w.y; bv[4 * q + 2] = w.z; bv[4 * q + 3] = w.w;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) bv[j] = (nb + j < N) ? ep.bias[nb + j] : 0.f;
+          }
+        }
         float mk[16];
         if (mode & EPI_RELU_BWD) {
           if (row_ok) load16_bf16(mrow, nb, N, true, mk);
@@ -224,7 +239,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           const int n = nb + j;
           const bool ok = row_ok && n < N;
           float x = v[j];
-          if (mode & EPI_BIAS) x += (n < N) ? ep.bias[n] : 0.f;
+          if (mode & EPI_BIAS) x += bv[j];
           if (mode & EPI_RELU) x = fmaxf(x, 0.f);
           if (mode & EPI_RELU_BWD) x = mk[j] > 0.f ? x : 0.f;
           if (mode & EPI_MSE) {
