@@ -174,16 +174,16 @@ def test_toggle_bits_and_stats_from_event_csr():
     assert np.array_equal(x2, want[2:5])
 
 
-@pytest.mark.parametrize("n_sel", [64, 70, 130])
+@pytest.mark.parametrize("n_sel", [64, 70, 130, 520])
 def test_dense_toggle_bits_of_windows_match_per_window_bits(n_sel):
     """gtp_toggle_bits_windows against gtp_toggle_bits window by window: an
-    odd net count (a partial last group of 64, an odd row stride), a window
+    odd net count (a partial last group of 256, an odd row stride), a window
     longer than one 2048-row chunk, events outside the windows, rows outside
     every window left as they were."""
     torch = _torch()
     from gtpower_b200 import proxy
     rng = np.random.default_rng(21 + n_sel)
-    tpc, n_net, n_cyc = 50, 300, 6000
+    tpc, n_net, n_cyc = 50, 600, 6000
     sel = torch.from_numpy(rng.choice(n_net, n_sel, replace=False).astype(np.int32)).cuda()
     windows, ref = [], torch.zeros((n_cyc, n_sel), dtype=torch.bfloat16, device="cuda")
     cuts = [100, 900, 3700, 3701, 5500]           # rows [0, 100) and [5500, 6000) belong to no window
