@@ -1083,9 +1083,23 @@ __global__ void tile_first_kernel(const KParams pv, const KParams* __restrict__ 
 
 // out[e] = glitch_pw of event e of its net, one warp per net. Parameters from
 // *pd when set (device memory), else from pv.
+//
+// The warp steps through the net's events 24 at a time: lane l holds event
+// e0 - 4 + l, lanes 4..27 own their events and lanes 0-3 and 28-31 show the
+// neighbours. Each lane finds its event's period group (the run of events in
+// one clock period; the waveform's first event g0 stands alone) from ballots
+// of the group starts and ends, and the flags and width of glitch_pw follow
+// from the group sizes of the lane and its neighbours. An owned event whose
+// group, or previous group, reaches the edge of the 32 events (five or more
+// events in one period) takes the per-event routine glitch_pw instead; both
+// give the same result.
 __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ pd, float* __restrict__ out) {
   const KParams& p = pd ? *pd : pv;
   const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  const unsigned below = lane == 31 ? full : ((1u << (lane + 1)) - 1u);  // lanes 0..lane
+  const unsigned above = ~((1u << lane) - 1u);                            // lanes lane..31
+  const bool owner = lane >= 4 && lane < 28;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t net = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; net < p.n_net;
        net += warps) {
@@ -1094,14 +1108,71 @@ __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ p
     if (p.net_glitch && !p.net_glitch[net]) continue;   // read by clock pins only: never a glitch
     const int64_t base = p.net_base ? p.net_base[net] : 0;
     const int64_t g0 = base == 0 ? lo : -1;
-    for (int64_t e = lo + lane; e < hi; e += 32) {
-      const int64_t t = ev_time(p.ev_t, e);
-      const int64_t cyc = div_floor_t(t, p.tpc, p.tpc_magic64);
-      const int64_t cs = cyc * p.tpc;
-      // an event alone in its period is never a glitch event
-      const bool prev_same = e - 1 >= lo && ev_time(p.ev_t, e - 1) >= cs;
-      const bool next_same = e + 1 < hi && ev_time(p.ev_t, e + 1) < cs + p.tpc;
-      out[e] = (prev_same || next_same) ? glitch_pw(p, e, lo, hi, g0, t, cs) : -1.0f;
+    for (int64_t e0 = lo; e0 < hi; e0 += 24) {
+      const int64_t e = e0 - 4 + lane;
+      const bool valid = e >= lo && e < hi;
+      const int64_t t = valid ? ev_time(p.ev_t, e) : 0;
+      const int64_t c = valid ? div_floor_t(t, p.tpc, p.tpc_magic64) : 0;
+      const int64_t t_prev = __shfl_up_sync(full, t, 1), c_prev = __shfl_up_sync(full, c, 1);
+      const int64_t t_next = __shfl_down_sync(full, t, 1), c_next = __shfl_down_sync(full, c, 1);
+      // period groups: g0 stands alone; past lane 0 and lane 31 a group is
+      // taken to go on (unknown)
+      const bool has_prev = valid && e != g0 && e - 1 >= lo && e - 1 != g0;
+      const bool has_next = valid && e != g0 && e + 1 < hi;
+      const bool join_prev = has_prev && (lane == 0 || c_prev == c);
+      const bool join_next = has_next && (lane == 31 || c_next == c);
+      const unsigned S = __ballot_sync(full, !join_prev);
+      const unsigned E = __ballot_sync(full, !join_next);
+      // first / last lane of this lane's group, -1 when it reaches outside
+      const int first = (S & below) ? 31 - __clz(S & below) : -1;
+      const int last = (E & above) ? __ffs(E & above) - 1 : -1;
+      const int first_prev = __shfl_up_sync(full, first, 1);
+      const int last_prev = __shfl_up_sync(full, last, 1);
+      const int last_next = __shfl_down_sync(full, last, 1);
+      if (!owner || !valid) continue;
+      float res = -1.0f;
+      bool slow = first < 0 || last < 0;
+      if (!slow && e != g0) {
+        const int k = last - first + 1;
+        const int lim = k >= 2 ? (k & ~1) : 0;
+        const int off = lane - first;
+        if (off < lim) {
+          int64_t w = -1;
+          if (e - 1 >= lo) {
+            bool pflag = false;
+            if (off > 0) {
+              pflag = true;
+            } else if (e - 1 != g0) {
+              // e - 1 ends the previous group: flagged when that group is even
+              if (first_prev <= 0) {
+                slow = true;  // it may reach before lane 0
+              } else {
+                const int kp = last_prev - first_prev + 1;
+                pflag = kp >= 2 && (kp & 1) == 0;
+              }
+            }
+            if (pflag) w = t - t_prev;
+          }
+          if (!slow && e + 1 < hi) {
+            bool nflag = false;
+            if (lane + 1 <= last) {
+              nflag = off + 1 < lim;
+            } else if (e + 2 < hi) {
+              // e + 1 starts the next group: flagged when it holds two or more
+              nflag = last_next < 0 || last_next >= lane + 2;
+            }
+            if (nflag) w = max(w, t_next - t);
+          }
+          if (w >= 0) res = __double2float_rn(__dmul_rn(static_cast<double>(w), p.ts));
+        }
+      }
+      if (slow) {
+        const int64_t cs = c * p.tpc;
+        const bool prev_same = e - 1 >= lo && t_prev >= cs;
+        const bool next_same = e + 1 < hi && t_next < cs + p.tpc;
+        res = (prev_same || next_same) ? glitch_pw(p, e, lo, hi, g0, t, cs) : -1.0f;
+      }
+      out[e] = res;
     }
   }
 }
