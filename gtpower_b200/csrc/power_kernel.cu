@@ -1188,7 +1188,7 @@ __device__ __forceinline__ int64_t lower_bound_time(const int64_t* __restrict__ 
   return lo;
 }
 
-// out[nets[w]] = the window's periodic pattern of net nets[w], one warp per
+// out[nets[w]] = the window's periodic pattern of net nets[w], one block per
 // net: its events in [TL, TH) = [max(t_lo, 1), min(t_hi, tmax + 1)) are edge
 // k0, k0 + 1, ... of the sequence whose edge k lies at (k / 2) * tpc + (k odd
 // ? pb : pa) with value (k odd ? v0 : 1 - v0), no edge of the sequence in
@@ -1198,12 +1198,11 @@ __device__ __forceinline__ int64_t lower_bound_time(const int64_t* __restrict__ 
 // takes the net's events one by one.
 __global__ void pclk_kernel(const KParams pv, const KParams* __restrict__ pd, const int32_t* __restrict__ nets,
                             int32_t n, int2* __restrict__ out) {
+  // one block per net: every thread reads the header, all check the events
   const KParams& p = pd ? *pd : pv;
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t w = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; w < n; w += warps) {
+  for (int64_t w = blockIdx.x; w < n; w += gridDim.x) {
     const int32_t net = nets[w];
-    if (net < 0 || net >= p.n_net) continue;
+    if (net < 0 || net >= p.n_net) continue;  // uniform over the block
     const int64_t lo = p.net_off[net], hi = p.net_off[net + 1];
     const int64_t tpc = p.tpc;
     bool ok = lo >= 0 && hi >= lo && hi <= p.n_event && tpc >= 2 && tpc < (int64_t(1) << 30);
@@ -1237,16 +1236,16 @@ __global__ void pclk_kernel(const KParams pv, const KParams* __restrict__ pd, co
       end_tmax = tn == p.tmax && p.tmax < TH;
       ok = ok && (km >> 1) * tpc + ((km & 1) ? pb : pa) < TL && (tn >= TH || end_tmax);
     }
+    bool good = true;
     if (ok) {
-      bool good = true;
-      for (int64_t j = lane; j < u - l; j += 32) {
+      for (int64_t j = threadIdx.x; j < u - l; j += blockDim.x) {
         const int64_t k = k0 + j;
         good = good && ev_time(p.ev_t, l + j) == (k >> 1) * tpc + ((k & 1) ? pb : pa) &&
                ev_value(p.ev_v, l + j) == ((k & 1) ? v0 : 1 - v0);
       }
-      ok = __all_sync(0xffffffffu, good);
     }
-    if (lane == 0)
+    ok = __syncthreads_and(ok && good) != 0;
+    if (threadIdx.x == 0)
       out[net] = ok ? make_int2(static_cast<int>(pa),
                                 static_cast<int>(static_cast<uint32_t>(pb) | (end_tmax ? (1u << 30) : 0u) |
                                                  (static_cast<uint32_t>(v0) << 31)))
@@ -1302,7 +1301,7 @@ cudaError_t launch_glitch_pw(const KParams& p, const KParams* d_p, float* out, c
 cudaError_t launch_pclk(const KParams& p, const KParams* d_p, const int32_t* nets, int32_t n, int2* out,
                         cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
-  const int blocks = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(n) * 32 + 255) / 256, 148 * 8));
+  const int blocks = static_cast<int>(std::min<int64_t>(n, 148 * 8));
   pclk_kernel<<<blocks, 256, 0, stream>>>(p, d_p, nets, n, out);
   return cudaGetLastError();
 }
