@@ -11,7 +11,7 @@
 4. Per-cycle toggle bits of the selected nets (gtp_toggle_bits) are the
    network's inputs; the BF16 MLP (gtp_proxy_*) trains on the labelled
    cycles and predicts the rest.
-5. The engine stays the judge: cycles whose input activity lies outside the
+5. The engine stays the authority: cycles whose input activity lies outside the
    training range and an audit sample are recomputed with it.
 
 Every step runs in libgtpb200.so kernels; torch tensors hold device memory and

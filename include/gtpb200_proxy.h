@@ -16,7 +16,7 @@
  * trained against per-cycle powers that the engine itself computes (mean
  * squared error on targets standardised per output, Adam). Weights and
  * activations are BF16 with FP32 accumulation on the tcgen05 tensor cores;
- * the master weights and Adam moments are FP32. The engine stays the judge:
+ * the master weights and Adam moments are FP32. The engine stays the authority:
  * callers audit a sample of cycles and recompute out-of-range ones with it.
  *
  * Pointers named d_ are device pointers on the proxy's device; all others
