@@ -120,3 +120,18 @@ def test_clock_runs_on_synthetic_flat_design():
     compare(a, ref)
     compare(b, ref)
     _same_dynamic(a, b)
+
+
+@pytest.mark.parametrize("threads,gates", [(128, 0), (64, 256), (256, 1024)])
+def test_clock_runs_block_shapes(threads, gates):
+    """Blocks of 64 or 128 threads (the run scan with 2 or 4 warps) and
+    several cells per thread (the run state and shared sums reset per
+    cell)."""
+    d, ev = _design(1)
+    ref = _oracle(d, ev)
+    a = _run(d, [ev], True, periodic=PERIODIC_ONE_WINDOW[1], cycles_per_tile=6, threads_per_block=threads,
+             gates_per_block=gates)
+    b = _run(d, [ev], False, cycles_per_tile=6, threads_per_block=threads, gates_per_block=gates)
+    compare(a, ref)
+    compare(b, ref)
+    _same_dynamic(a, b)
