@@ -85,6 +85,17 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(pg, values, device):
+    """Each value's maximum over the ranks (the slowest rank's time); pg is
+    torch.distributed or None for one process."""
+    if pg is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return t.tolist()
+
+
 def workload(args, rank: int):
     from gtpower_b200 import synth
     spec = synth.FlatSpec(n_cell=args.cells, n_cycle=args.cycles, seed=20261203 + 1)
@@ -708,10 +719,7 @@ def main():
     e2e_ms = float(np.mean(e2e_ms_list))
 
     # max over ranks
-    if pg:
-        t = torch.tensor([step_ms, e2e_ms, walk_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        step_ms, e2e_ms, walk_ms = t.tolist()
+    step_ms, e2e_ms, walk_ms = max_over_ranks(pg, [step_ms, e2e_ms, walk_ms], "cuda")
 
     d2h = 4 * 5 * design.n_cell + 4 * 5 * eng.n_period + 8 * 5 * 6 + 4
     b_alg = algorithmic_bytes(design, n_event)

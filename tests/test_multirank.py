@@ -1,0 +1,63 @@
+"""The multi-process path of bench.py, run on the CPU as two gloo ranks: the
+timing reduction keeps the slowest rank's time, every rank evaluates its own
+trace of the same design (weak scaling, no data-path collective), and the
+reference arm does its work on rank 0 only."""
+import datetime
+import os
+import socket
+import types
+
+import pytest
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import bench
+        assert bench.dist_env() == (rank, world, rank)
+        slowest = bench.max_over_ranks(dist, [1.0 + rank, 10.0 - rank, 3.0], "cpu")
+        design, _, trace = bench.workload(types.SimpleNamespace(cells=300, cycles=20), rank)
+        ev = trace.full()
+        mine = torch.tensor([float(design.n_cell), float(design.n_pin), float(ev.n_event),
+                             float(ev.time.sum() % 1_000_003)], dtype=torch.float64)
+        all_ranks = [torch.zeros(4, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(all_ranks, mine)
+        if rank != 0:
+            assert bench.run_reference(types.SimpleNamespace(), rank, world) is None
+        q.put((rank, slowest, [t.tolist() for t in all_ranks]))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_reduce_times_and_walk_their_own_traces():
+    mp = pytest.importorskip("torch.multiprocessing")
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    mp.spawn(_rank_main, args=(2, _free_port(), q), nprocs=2, join=True)
+    res = {}
+    for _ in range(2):
+        rank, slowest, all_ranks = q.get()
+        res[rank] = (slowest, all_ranks)
+    assert sorted(res) == [0, 1]
+    for rank in (0, 1):
+        slowest, (r0, r1) = res[rank]
+        assert slowest == [2.0, 10.0, 3.0]  # each value's maximum over the two ranks
+        assert r0[:2] == r1[:2]             # the same design on both ranks
+        assert r0[2:] != r1[2:]             # each rank its own trace
+    assert res[0][1] == res[1][1]
+
+
+def test_max_over_ranks_without_a_process_group():
+    import bench
+    assert bench.max_over_ranks(None, [3, 1.5], "cpu") == [3.0, 1.5]
