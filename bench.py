@@ -31,7 +31,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "net events/s (time-based power walk, flat synthetic 200k cells x 10k cycles)"
+def metric_name(cells: int, cycles: int) -> str:
+    """The flat workload's metric, named by its size (200k cells x 10k cycles by default)."""
+    def k(n: int) -> str:
+        return f"{n // 1000}k" if n % 1000 == 0 else str(n)
+    return f"net events/s (time-based power walk, flat synthetic {k(cells)} cells x {k(cycles)} cycles)"
 UNIT = "events/s"
 
 
@@ -565,7 +569,7 @@ def run_reference(args, rank, world):
     job_s = [t * tpe / max(pe, 1) for t, pe in zip(secs, pes)]
     ms = float(np.mean(job_s)) * 1e3
     value = total_events / (ms / 1e3)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    line = {"metric": metric_name(args.cells, args.cycles), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
@@ -742,7 +746,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC,
+            "metric": metric_name(args.cells, args.cycles),
             "value": world * n_event / (step_ms / 1e3),
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",

@@ -61,3 +61,10 @@ def test_two_gloo_ranks_reduce_times_and_walk_their_own_traces():
 def test_max_over_ranks_without_a_process_group():
     import bench
     assert bench.max_over_ranks(None, [3, 1.5], "cpu") == [3.0, 1.5]
+
+
+def test_metric_names_the_workload_size():
+    import bench
+    assert bench.metric_name(200_000, 10_000) == \
+        "net events/s (time-based power walk, flat synthetic 200k cells x 10k cycles)"
+    assert bench.metric_name(2000, 50) == "net events/s (time-based power walk, flat synthetic 2k cells x 50 cycles)"
