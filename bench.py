@@ -39,6 +39,12 @@ def metric_name(cells: int, cycles: int) -> str:
 UNIT = "events/s"
 
 
+def workload_name(args) -> str:
+    """The default workload's description, the same on the engine's line and the reference arm's."""
+    return (f"flat synthetic sky130hd {args.cells} cells x {args.cycles} cycles "
+            "(2 ns, 1 ps ticks, toggle U[0.05,0.3], glitch p=0.05)")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -47,8 +53,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=200_000)
     ap.add_argument("--cycles", type=int, default=10_000)
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity leg (the timed configuration's outputs against the FP64 oracle)")
     ap.add_argument("--cycles-per-tile", type=int, default=0)
     ap.add_argument("--e2e-split", default="ramp", choices=["ramp", "even"],
                     help="e2e windows: 'ramp' grows them 1.5x each (a short first copy, then each copy "
@@ -512,33 +519,85 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(design, ev, sample_seconds: float, total_events: int, total_pin_events: int):
-    """FP32 restatement of the reference CPU path on a bounded cell sample,
-    all host threads; extrapolated to net events/s of the whole trace."""
+def cpu_baseline(design, ev, total_events: int):
+    """The FP32 restatement of the reference CPU path (power/Power.cc:227-386:
+    static cell split over a thread pool, per-thread per-cycle arrays) over
+    every cell of the trace, on all host threads: a measured duration of the
+    whole workload, not an extrapolation."""
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
-    rng = np.random.default_rng(7)
-    order = rng.permutation(design.n_cell).astype(np.int32)
-    cnt = np.diff(ev.net_off)
-    cell_pin_ev = np.add.reduceat(
-        np.where(design.pin_net >= 0, cnt[np.maximum(design.pin_net, 0)], 0), design.cell_pin_off[:-1])
-    # calibrate on a small slice, then size the sample to ~sample_seconds
-    k0 = max(threads * 4, 200)
-    r0 = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
-    pe0 = int(cell_pin_ev[order[:k0]].sum())
-    rate = pe0 / max(r0.seconds, 1e-6)
-    k = int(min(design.n_cell, max(k0, k0 * sample_seconds / max(r0.seconds, 1e-6))))
-    r = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k], outputs=False)
-    pe = int(cell_pin_ev[order[:k]].sum())
-    frac = pe / max(total_pin_events, 1)
-    ev_per_s = total_events * frac / max(r.seconds, 1e-9)
-    return {"value": ev_per_s, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"{k} of {design.n_cell} cells (random), {pe} of {total_pin_events} pin events, "
-                       f"{r.seconds:.2f} s on {threads} threads; extrapolated by pin-event share"),
+    r = orc.run(design, ev, fp32=True, threads=threads, outputs=False)
+    return {"value": total_events / max(r.seconds, 1e-9), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the whole workload: all {design.n_cell} cells, {total_events} net events, "
+                      f"{r.seconds:.2f} s on {threads} threads (per-pin slews and arc delays "
+                      "precomputed, where the reference queries its timing graph per event)",
             "seconds": r.seconds}
 
 
+def _rel_errors(got: np.ndarray, ref: np.ndarray, floor: float = 1e-3) -> dict:
+    """Largest relative error of got against ref per column (quantity), over
+    the values above floor x the column's largest magnitude, and the largest
+    error of the rest relative to that magnitude (sums that cancel to near
+    zero are held to the column scale)."""
+    got = np.asarray(got, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    out = {}
+    names = ["leakage", "internal", "glitch_internal", "switching", "glitch_switching"]
+    for q in range(ref.shape[1]):
+        g, r = got[:, q], ref[:, q]
+        scale = float(np.max(np.abs(r))) if r.size else 0.0
+        big = np.abs(r) > floor * scale
+        rel = float(np.max(np.abs(g[big] - r[big]) / np.abs(r[big]))) if big.any() else 0.0
+        small = float(np.max(np.abs(g[~big] - r[~big])) / scale) if (~big).any() and scale > 0 else 0.0
+        out[names[q]] = {"max_rel": rel, "small_max_abs_over_scale": small}
+    return out
+
+
+def parity_leg(design, ev, results: dict, counts_res, threads: int) -> dict:
+    """The engine's outputs of the timed configuration against an FP64
+    re-evaluation of the reference CPU path (the oracle) over the whole
+    trace: integer counts bit for bit, and the relative error of every
+    reported quantity per cell, per cycle and in the totals."""
+    from oracle import oracle as orc
+    ref = orc.run(design, ev, fp32=False, threads=threads)
+    # cell5 columns: internal, glitch internal, switching, glitch switching, leakage
+    # (internal and switching without glitch); in the oracle's order of cycle5
+    perm = [4, 0, 1, 2, 3]
+    out = {"oracle": f"FP64 restatement of the reference CPU path over all {design.n_cell} cells",
+           "oracle_seconds": ref.seconds, "tolerance": "1e-5 relative (values under 1e-3 of their "
+           "column's largest magnitude: 1e-8 of it)"}
+    ok = True
+    for name, res in results.items():
+        cell = _rel_errors(res.cell5[:, perm], ref.cell5[:, perm])
+        cyc = _rel_errors(res.cycle5.T, ref.cycle5.T)
+        tot = {k: float(abs(res.totals[q] - ref.totals[q]) / max(abs(ref.totals[q]), 1e-300))
+               for q, k in enumerate(["leakage", "internal", "glitch_internal", "switching", "glitch_switching"])}
+        worst = max([v["max_rel"] for v in cell.values()] + [v["max_rel"] for v in cyc.values()]
+                    + list(tot.values()))
+        worst_small = max([v["small_max_abs_over_scale"] for v in cell.values()]
+                          + [v["small_max_abs_over_scale"] for v in cyc.values()])
+        ok = ok and worst <= 1e-5 and worst_small <= 1e-8
+        out[name] = {"cell": cell, "cycle": cyc, "totals": tot, "max_rel": worst}
+    if counts_res is not None:
+        c = counts_res.counts
+        fields = ("cell_events", "cell_glitches", "cell_half_toggles", "cell_related",
+                  "cycle_events", "cycle_glitches")
+        mism = {f: int(np.count_nonzero(getattr(c, f).astype(np.int64) != getattr(ref, f).astype(np.int64)))
+                for f in fields}
+        out["counts_exact"] = all(v == 0 for v in mism.values()) and c.dropped == ref.dropped
+        out["count_mismatches"] = mism
+        out["pin_events_counted"] = int(c.cell_events.astype(np.int64).sum())
+        out["glitch_events_counted"] = int(c.cell_glitches.astype(np.int64).sum())
+        ok = ok and out["counts_exact"]
+    out["pass"] = bool(ok)
+    return out
+
+
 def run_reference(args, rank, world):
+    """The reference arm: the FP32 restatement of the reference CPU path
+    (the reference's own build needs Tcl, SWIG, flex, bison, Eigen3 and CUDD,
+    which this image lacks) over every cell of the same trace in each timed
+    step, on all host threads. Warm-up steps walk a small cell sample."""
     if rank != 0:
         return
     design, info, trace = workload(args, 0)
@@ -548,36 +607,25 @@ def run_reference(args, rank, world):
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(11)
-    order = rng.permutation(design.n_cell).astype(np.int32)
-    cnt = np.diff(ev.net_off)
-    cell_pin_ev = np.add.reduceat(
-        np.where(design.pin_net >= 0, cnt[np.maximum(design.pin_net, 0)], 0), design.cell_pin_off[:-1])
-    # size each step's sample to ~10 s of host work
-    k0 = max(threads * 4, 200)
-    r0 = orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
-    k = int(min(design.n_cell, max(k0, k0 * 10.0 / max(r0.seconds, 1e-6))))
-    for w in range(args.warmup):
-        orc.run(design, ev, fp32=True, threads=threads, cells=order[:k0], outputs=False)
+    warm = rng.permutation(design.n_cell)[:max(threads * 4, 2000)].astype(np.int32)
+    for _ in range(args.warmup):
+        orc.run(design, ev, fp32=True, threads=threads, cells=warm, outputs=False)
     secs = []
-    pes = []
-    for s in range(args.steps):
-        sel = np.roll(order, -s * k)[:k]
-        r = orc.run(design, ev, fp32=True, threads=threads, cells=sel, outputs=False)
+    for _ in range(args.steps):
+        r = orc.run(design, ev, fp32=True, threads=threads, outputs=False)
         secs.append(r.seconds)
-        pes.append(int(cell_pin_ev[sel].sum()))
-    # whole-job time = sample time scaled by pin-event share
-    job_s = [t * tpe / max(pe, 1) for t, pe in zip(secs, pes)]
-    ms = float(np.mean(job_s)) * 1e3
+    ms = float(np.mean(secs)) * 1e3
     value = total_events / (ms / 1e3)
-    line = {"metric": metric_name(args.cells, args.cycles), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+    line = {"metric": metric_name(args.cells, args.cycles), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"flat synthetic sky130hd {args.cells} cells x {args.cycles} cycles",
-                       "n_event": total_events, "pin_events": tpe},
+            "config": {"workload": workload_name(args), "n_event": total_events, "pin_events": tpe},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{k} random cells per step ({np.mean(pes):.3g} pin events), "
-                                       f"extrapolated by pin-event share"},
+                             "sample": f"the whole workload each timed step: all {design.n_cell} cells, "
+                                       f"{total_events} net events; warm-up steps walk {warm.shape[0]} cells; "
+                                       "per-pin slews and arc delays precomputed (the reference queries "
+                                       "its timing graph per event)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -674,7 +722,9 @@ def main():
         ev1.record(stream)
         return ev0, ev1
 
-    launches_per_step = 1 + 2  # walk (one bucket here) + 2 finalize kernels
+    # per step: tile_first, glitch_pw, pclk, work_keys (then the library's
+    # radix sort), the walk (one pin bucket here), finalize_cells, finalize_cycles
+    launches_per_step = 7
     from gtpower_b200 import _abi
     import ctypes as C
 
@@ -739,10 +789,27 @@ def main():
         except Exception:
             traffic = None
 
+    # results of the timed configuration for the parity leg: the
+    # device-resident single window and the host-pushed windows of the e2e leg
+    res_e2e = res
+    device_step()
+    res_dev = eng.fetch()
+    counts_res = None
+    if rank == 0 and not args.no_parity:
+        with B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
+                       gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
+                       clock_runs=not args.no_clock_runs, collect_counts=True) as ceng:
+            ceng.push_device(n_event, d_off.data_ptr(), d_t.data_ptr(), d_v.data_ptr())
+            counts_res = ceng.fetch(counts=True)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(design, ev, args.cpu_sample_seconds, n_event, tpe)
+        cpu = cpu_baseline(design, ev, n_event)
         cpu.pop("seconds", None)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_leg(design, ev, {"device_resident": res_dev, f"e2e_{len(e2e_wins)}_windows": res_e2e},
+                            counts_res, os.cpu_count() or 1)
 
     if rank == 0:
         line = {
@@ -751,8 +818,7 @@ def main():
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"flat synthetic sky130hd {args.cells} cells x {args.cycles} cycles "
-                                   f"(2 ns, 1 ps ticks, toggle U[0.05,0.3], glitch p=0.05)",
+            "config": {"workload": workload_name(args),
                        "n_event": n_event, "pin_events": tpe, "n_cell": design.n_cell,
                        "n_pin": design.n_pin, "n_net": design.n_net, "n_period": eng.n_period,
                        "cell_cycles_per_s": world * design.n_cell * eng.n_period / (step_ms / 1e3),
@@ -768,6 +834,7 @@ def main():
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "algorithmic_bytes_per_launch": b_alg, "kernel": "power_walk_kernel"},
             "cpu_baseline": cpu,
+            "parity": parity,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
             "totals_w": {"leakage": float(res.totals[0]), "internal": float(res.totals[1]),

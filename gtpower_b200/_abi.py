@@ -127,7 +127,7 @@ EXPORTED = sorted([
     "gtp_proxy_set_training_data", "gtp_proxy_get_norm", "gtp_proxy_train",
     "gtp_proxy_compute_grads", "gtp_proxy_adam_step", "gtp_proxy_get_params",
     "gtp_proxy_set_params", "gtp_proxy_get_grads", "gtp_proxy_predict", "gtp_toggle_bits", "gtp_toggle_bits_windows",
-    "gtp_net_toggle_stats", "gtp_bf16_gemm",
+    "gtp_net_toggle_stats", "gtp_bf16_gemm", "gtp_bf16_gemm_checked",
 ])
 
 _lib = None
@@ -226,6 +226,7 @@ def _bind_proxy(L: C.CDLL) -> None:
         "gtp_toggle_bits_windows": ([C.POINTER(gtp_bits_window), i32, _P, i32, i64, i64, _P, i64, _P], i32),
         "gtp_net_toggle_stats": ([_P, _P, i32, i64, i64, i64, _P, _P, _P, _P], i32),
         "gtp_bf16_gemm": ([_P, i64, _P, i64, i64, i64, i64, _P, i32, _P, i64, _P], i32),
+        "gtp_bf16_gemm_checked": ([_P, i64, _P, i64, i64, i64, i64, _P, i32, _P, i64, i64, i32, _P, _P], i32),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

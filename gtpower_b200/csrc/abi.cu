@@ -1241,6 +1241,10 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   // accumulators must start at zero
   e = cudaMemsetAsync(s, 0, off_tg, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: clear");
+  // the context's status word reports this call's events only (a 4-byte
+  // memset of memory the context already holds, not an allocation)
+  e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: status clear");
 
   KParams k = make_params(c);
   k.cell_acc = reinterpret_cast<double*>(s + off_cell);

@@ -1013,4 +1013,29 @@ gtp_status gtp_bf16_gemm(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, 
   return e == cudaSuccess ? GTP_OK : GTP_ECUDA;
 }
 
+gtp_status gtp_bf16_gemm_checked(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int64_t m,
+                                 int64_t n, int64_t k, const float* d_bias, int32_t relu, float* d_c, int64_t ldc,
+                                 int64_t spin_limit_cycles, int32_t test_skip_load_block, int32_t* d_err,
+                                 void* stream) {
+  if (d_err == nullptr || spin_limit_cycles < 0 || test_skip_load_block < -1) return GTP_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(d_err, 0, sizeof(int32_t), s) != cudaSuccess) return GTP_ECUDA;
+  Epilogue ep;
+  ep.mode = U::EPI_OUT_F32 | (d_bias ? U::EPI_BIAS : 0) | (relu ? U::EPI_RELU : 0);
+  ep.bias = d_bias;
+  ep.out_f = d_c;
+  ep.ldf = ldc;
+  ep.err = d_err;
+  ep.spin_limit = spin_limit_cycles;
+  ep.skip_load_block = test_skip_load_block;
+  cudaError_t e = U::gemm_bf16_tn(Operand{d_a, m, lda}, Operand{d_b, n, ldb}, m, n, k, ep, s);
+  if (e == cudaErrorInvalidValue) return GTP_EINVAL;
+  if (e != cudaSuccess) return GTP_ECUDA;
+  int32_t h = 0;
+  e = cudaMemcpyAsync(&h, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return GTP_ECUDA;
+  return h != 0 ? GTP_ETIMEOUT : GTP_OK;
+}
+
 }  // extern "C"

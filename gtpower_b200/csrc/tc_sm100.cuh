@@ -16,8 +16,9 @@
 namespace gtpb {
 namespace tc {
 
-// Longest a single wait may spin before the kernel gives up, in SM clock
-// cycles (about one second at 2 GHz).
+// Default longest spin of a single wait before the kernel gives up, in SM
+// clock cycles (about one second at 2 GHz). Kernels take the limit as a
+// parameter so that a caller (or a test) can shorten it.
 constexpr long long kSpinLimit = 2000000000LL;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -56,12 +57,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for the phase with the given parity to complete. Returns false when
-// `abort` (shared, may be null) becomes non-zero or the spin limit passes.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort) {
+// `abort` (shared, may be null) becomes non-zero or `limit` SM clock cycles
+// pass.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort,
+                                          long long limit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
     if (abort != nullptr && *abort) return false;
-    if (clock64() - t0 > kSpinLimit) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }

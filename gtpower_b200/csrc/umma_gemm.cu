@@ -17,9 +17,11 @@
 //                      fused epilogue and returns the accumulator, so that
 //                      the next tile's MMAs overlap this tile's stores.
 // A 4-stage ring of mbarriers (full: TMA bytes landed; empty: MMAs that read
-// the stage are done) overlaps loads with math. Every wait is bounded: on
-// timeout the kernel records an error bit, lets its own copies in flight
-// land, frees TMEM and returns.
+// the stage are done) overlaps loads with math. Every wait is bounded (by
+// Epilogue::spin_limit): on timeout the kernel records an error bit; before
+// it returns, the producer waits for the copies it issued to land and the
+// MMA issuer for the MMAs it issued to finish, so that neither shared memory
+// nor TMEM (freed last) is released under work in flight.
 #include "tc_sm100.cuh"
 #include "umma_gemm.h"
 
@@ -88,13 +90,15 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* empty = full + STAGES;
   uint64_t* acc_full = empty + STAGES;   // [2] accumulator ready for the epilogue
   uint64_t* acc_empty = acc_full + 2;    // [2] accumulator drained by the epilogue
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  uint64_t* mma_done = acc_empty + 2;    // every MMA this CTA issued is complete
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
   volatile int* abort_v = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = (K + BK - 1) / BK;
   const int tiles_n = (N + BN - 1) / BN;
   const int n_tiles = ((M + BM - 1) / BM) * tiles_n;
+  const long long spin = ep.spin_limit > 0 ? ep.spin_limit : tc::kSpinLimit;
 
   if (threadIdx.x == 0) {
     tc::tma_prefetch_desc(&tmA);
@@ -107,6 +111,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       tc::mbar_init(&acc_full[a], 1);
       tc::mbar_init(&acc_empty[a], EPI_WARPS);
     }
+    tc::mbar_init(mma_done, 1);
     *abort_v = 0;
     tc::mbar_init_fence();
   }
@@ -122,28 +127,31 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (warp == 0) {
     // TMA producer: one stage ring across all of this CTA's tiles
     if (lane == 0) {
-      int64_t g = 0, issued = 0;
+      const int64_t skip = blockIdx.x == 0 ? ep.skip_load_block : -1;
+      int64_t g = 0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_v; t += gridDim.x) {
         const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = static_cast<int>(g % STAGES);
-          if (g >= STAGES && !tc::mbar_wait(&empty[s], static_cast<uint32_t>(((g / STAGES) - 1) & 1), abort_v)) {
+          if (g >= STAGES &&
+              !tc::mbar_wait(&empty[s], static_cast<uint32_t>(((g / STAGES) - 1) & 1), abort_v, spin)) {
             *abort_v = 1;
             if (ep.err) atomicOr(ep.err, 1);
             break;
           }
+          if (g == skip) continue;  // timeout-path test: this stage's bytes never arrive
           uint8_t* a = smem + s * C::STAGE;
           uint8_t* b = a + C::A_BYTES;
           tc::mbar_expect_tx(&full[s], C::STAGE);
           tc::tma_load_2d(a, &tmA, &full[s], kb * BK, m0);
           tc::tma_load_2d(b, &tmB, &full[s], kb * BK, n0);
-          issued = g + 1;
         }
+        if (*abort_v) break;
       }
-      if (*abort_v) {  // let this CTA's copies in flight land before exit
-        for (int64_t q = issued > STAGES ? issued - STAGES : 0; q < issued; ++q)
-          tc::mbar_wait(&full[q % STAGES], static_cast<uint32_t>((q / STAGES) & 1), nullptr);
-      }
+      // the last copies issued (one per stage at most) must land before the
+      // CTA exits; consumed stages pass at once
+      for (int64_t q = g > STAGES ? g - STAGES : 0; q < g; ++q)
+        if (q != skip) tc::mbar_wait(&full[q % STAGES], static_cast<uint32_t>((q / STAGES) & 1), nullptr, spin);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -156,11 +164,12 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int acc = i & 1;
         const uint32_t d = tmem + static_cast<uint32_t>(acc * BN);
         bool ok = !*abort_v;
-        if (ok && i >= 2 && !tc::mbar_wait(&acc_empty[acc], static_cast<uint32_t>(((i / 2) - 1) & 1), abort_v))
+        if (ok && i >= 2 &&
+            !tc::mbar_wait(&acc_empty[acc], static_cast<uint32_t>(((i / 2) - 1) & 1), abort_v, spin))
           ok = false;
         for (int kb = 0; ok && kb < nk; ++kb, ++g) {
           const int s = static_cast<int>(g % STAGES);
-          if (!tc::mbar_wait(&full[s], static_cast<uint32_t>((g / STAGES) & 1), abort_v)) {
+          if (!tc::mbar_wait(&full[s], static_cast<uint32_t>((g / STAGES) & 1), abort_v, spin)) {
             ok = false;
             break;
           }
@@ -182,6 +191,9 @@ __global__ void __launch_bounds__(THREADS, 1)
           break;
         }
       }
+      // TMEM is freed only after every MMA issued here is complete
+      tc::umma_commit(mma_done);
+      if (!tc::mbar_wait(mma_done, 0u, nullptr, spin) && ep.err) atomicOr(ep.err, 1);
     }
     __syncwarp();
   } else {
@@ -191,7 +203,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++i) {
       const int acc = i & 1;
       int acc_ok = 1;
-      if (lane == 0) acc_ok = tc::mbar_wait(&acc_full[acc], static_cast<uint32_t>((i / 2) & 1), nullptr) ? 1 : 0;
+      if (lane == 0) acc_ok = tc::mbar_wait(&acc_full[acc], static_cast<uint32_t>((i / 2) & 1), nullptr, spin) ? 1 : 0;
       acc_ok = __shfl_sync(0xffffffffu, acc_ok, 0);
       tc::tc_fence_after();
       if (!acc_ok) {

@@ -46,6 +46,12 @@ struct Epilogue {
   float* colsum = nullptr;
   float* loss = nullptr;  // += sum of squared errors under EPI_MSE
   int* err = nullptr;     // bit 1: a pipeline wait timed out
+  // longest spin of one pipeline wait, SM clock cycles; 0 = about one second
+  long long spin_limit = 0;
+  // test of the timeout path, -1 in normal use: the first CTA's TMA producer
+  // skips the loads of its k-th K block (counted over its tiles), so the MMA
+  // issuer's wait for them runs out after spin_limit
+  int skip_load_block = -1;
 };
 
 // Row-major bf16 matrix [rows, ld] whose first `k` columns are the K extent.

@@ -315,11 +315,15 @@ gtp_status  gtp_clock_run_nets(gtp_ctx* ctx, int32_t* n_clock_nets, int32_t* n_p
  * accumulators live in a 16 MiB static device array that every GPU loading
  * the library holds until exit. Limit: 40 bytes per cell + 56 per cycle
  * within 16 MiB (about 300k cells x 20k cycles); larger designs get
- * GTP_EOVERFLOW. The first call on a device looks up the array's address;
- * make that first call before any stream capture. All calls share the array
- * (each clears what it uses first), so calls that overlap on the GPU race.
- * Work is queued on the context's stream; gtp_sync waits and reports
- * invalid events. */
+ * GTP_EOVERFLOW. The first call on a device looks up the array's address
+ * and keeps it for the life of the process; make that first call before any
+ * stream capture, and after a cudaDeviceReset do not call this entry point
+ * again on that device in the same process (the kept address is stale). All
+ * calls share the array (each clears what it uses first), so calls that
+ * overlap on the GPU race. Work is queued on the context's stream; each call
+ * first clears the context's status word (dropping any unreported error of
+ * earlier work on the context), and gtp_sync then waits and reports this
+ * call's invalid events. */
 gtp_status  gtp_evaluate_noalloc(gtp_ctx* ctx, const gtp_events* d_ev, float* d_cell5,
                                  float* d_cycle5, double* d_totals);
 

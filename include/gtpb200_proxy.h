@@ -139,6 +139,21 @@ gtp_status  gtp_bf16_gemm(const uint16_t* d_a, int64_t lda, const uint16_t* d_b,
                           int64_t m, int64_t n, int64_t k, const float* d_bias, int32_t relu,
                           float* d_c, int64_t ldc, void* stream);
 
+/* gtp_bf16_gemm that reports its pipeline's health and waits for the result.
+ * Every wait inside the kernel (TMA bytes landed, MMAs done, accumulator
+ * drained) gives up after spin_limit_cycles SM clock cycles (0: about one
+ * second); a wait that gives up sets *d_err (a caller device int32, cleared
+ * first), the kernel lets its copies and MMAs in flight finish, frees its
+ * TMEM and returns, and the call returns GTP_ETIMEOUT (d_c is then
+ * unspecified). The device stays usable. test_skip_load_block >= 0 is a test
+ * of that path: the first CTA's TMA producer skips the loads of its K block
+ * with that index (counted over its tiles), so that the MMA issuer's wait
+ * for them runs out; -1 in normal use. Synchronises `stream`. */
+gtp_status  gtp_bf16_gemm_checked(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb,
+                                  int64_t m, int64_t n, int64_t k, const float* d_bias, int32_t relu,
+                                  float* d_c, int64_t ldc, int64_t spin_limit_cycles,
+                                  int32_t test_skip_load_block, int32_t* d_err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,3 +76,53 @@ def test_noalloc_rejects_design_beyond_scratch():
         st = _abi.lib().gtp_evaluate_noalloc(eng.ctx, C.byref(e), None, None, None)
         assert st == _abi.GTP_EOVERFLOW
         assert "scratch" in _abi.lib().gtp_last_error(eng.ctx).decode()
+
+
+def test_noalloc_reports_invalid_events_then_runs_clean():
+    """A trace whose times step back within a net makes gtp_sync report
+    GTP_EINVAL after the allocation-free call; the next call with a valid
+    trace starts from a clear status word and matches the regular path."""
+    import torch
+    from gtpower_b200 import B200Power, _abi, synth
+    from tests.parity import close
+
+    d, info = synth.flat_design(synth.FlatSpec(n_cell=2000, n_cycle=80, seed=31))
+    ev = synth.Trace(d, info, synth.TraceSpec(), seed=32).full()
+    read = np.zeros(d.n_net, dtype=bool)
+    read[d.pin_net[d.pin_net >= 0]] = True
+    counts = np.diff(ev.net_off)
+    net = int(np.nonzero(read & (counts >= 4) & (np.arange(d.n_net) != info["clock_net"]))[0][0])
+    a = int(ev.net_off[net])
+    bad_t = ev.time.copy()
+    bad_t[a + 1], bad_t[a + 2] = bad_t[a + 2], bad_t[a + 1]
+    dev = torch.device("cuda", 0)
+    with B200Power(d, device=0) as eng:
+        eng.read_power_activities(ev)
+        ref = eng.fetch()
+        L = _abi.lib()
+        npd = eng.n_period
+        cell5 = torch.zeros((d.n_cell, 5), dtype=torch.float32, device=dev)
+        cyc5 = torch.zeros((5, npd), dtype=torch.float32, device=dev)
+        d_off = torch.from_numpy(ev.net_off).to(dev)
+        d_v = torch.from_numpy(ev.packed.view(np.int32)).to(dev)
+        for times, ok in ((bad_t, False), (ev.time, True)):
+            d_t = torch.from_numpy(np.ascontiguousarray(times)).to(dev)
+            e = _abi.gtp_events()
+            e.n_event = ev.n_event
+            e.net_off = d_off.data_ptr()
+            e.time = d_t.data_ptr()
+            e.value_packed = d_v.data_ptr()
+            e.net_base = None
+            e.t_lo = 0
+            e.t_hi = np.iinfo(np.int64).max
+            _abi.check(L.gtp_evaluate_noalloc(eng.ctx, C.byref(e), cell5.data_ptr(), cyc5.data_ptr(), None),
+                       eng.ctx)
+            if not ok:
+                with pytest.raises(_abi.GtpError) as ex:
+                    eng.sync()
+                assert ex.value.status == _abi.GTP_EINVAL
+                assert "strictly increasing" in str(ex.value)
+            else:
+                eng.sync()
+                close("cell5", cell5.cpu().numpy(), ref.cell5, rtol=1e-6)
+                close("cycle5", cyc5.cpu().numpy().T, ref.cycle5.T, rtol=1e-6)
