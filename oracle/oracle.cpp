@@ -33,10 +33,14 @@
 //   Real = float  : the reference's own FP32 types (util/Types.hh), used as
 //                   the timed CPU baseline ("port" of the reference CPU path).
 //
-// Parity status: the reference cannot be built in this container (Tcl, SWIG,
-// flex, bison, Eigen3, CUDD absent), so this restatement is pinned against
-// hand-derived known-answer cases in tests/test_oracle_kat.py, not against
-// outputs of the reference binary.
+// Parity status: the reference binary cannot be built in this container
+// (Tcl, SWIG, flex, bison, Eigen3, CUDD absent). The restatement is pinned
+// (a) helper by helper against the reference's own table interpolation,
+// toggle, rise, cycle-index and glitch-ratio functions compiled from its
+// sources (oracle/Makefile target `ref`, tests/test_oracle_ref.py, and the
+// vectors they produced in tests/golden/ref_vectors.npz), (b) on the walk as a
+// whole by hand-derived known-answer cases (tests/test_oracle_kat.py) and the
+// reference's GCD example report (tests/test_gcd.py).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -696,6 +700,68 @@ int oracle_run(const gtp_design* d, const gtp_events* ev, const int32_t* cells,
   const auto t1 = std::chrono::steady_clock::now();
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   return rc;
+}
+
+// ---- single helpers of the restatement, checked one by one against the
+// reference's own functions compiled from its sources (oracle/_ref) ----
+
+// Engine::tableValue of one table: order 1 over the slew axis, order 2 over
+// (slew, load cap); values row-major [n1][n2]; scale 1. fp32 = 0: the FP64
+// interpolation; fp32 = 1: rounded to float as Table*::findValue returns.
+double oracle_table_value(int32_t order, int32_t n1, const float* axis1, int32_t n2, const float* axis2,
+                          const float* values, float slew, float cap, int fp32) {
+  std::vector<float> pool;
+  gtp_table tb{};
+  tb.order = order;
+  tb.axis1_var = order >= 1 ? GTP_AXIS_SLEW : GTP_AXIS_NONE;
+  tb.axis2_var = order >= 2 ? GTP_AXIS_CAP : GTP_AXIS_NONE;
+  tb.n1 = order >= 1 ? n1 : 1;
+  tb.n2 = order >= 2 ? n2 : 1;
+  tb.axis1_off = 0;
+  if (order >= 1) pool.insert(pool.end(), axis1, axis1 + n1);
+  tb.axis2_off = static_cast<int64_t>(pool.size());
+  if (order >= 2) pool.insert(pool.end(), axis2, axis2 + n2);
+  tb.value_off = static_cast<int64_t>(pool.size());
+  pool.insert(pool.end(), values, values + static_cast<int64_t>(tb.n1) * tb.n2);
+  tb.scale = 1.0f;
+  gtp_design d{};
+  d.timescale = 1e-12;
+  d.clk_period = 1e-9f;
+  d.tables = &tb;
+  d.n_table = 1;
+  d.lut_pool = pool.data();
+  d.lut_pool_len = static_cast<int64_t>(pool.size());
+  gtp_events ev{};
+  if (fp32) return static_cast<double>(Engine<float>(d, ev, 16).tableValue(0, slew, cap));
+  return Engine<double>(d, ev, 16).tableValue(0, slew, cap);
+}
+
+// findValueIndex over axis[0..n) at x.
+int64_t oracle_find_value_index(const float* axis, int32_t n, float x) {
+  return static_cast<int64_t>(Engine<double>::findValueIndex(x, axis, n));
+}
+
+// Cycle of tick t (clkedWaveformIdx as the oracle evaluates it).
+int64_t oracle_cycle_of(int64_t t, double timescale, float clk_period) {
+  gtp_design d{};
+  d.timescale = timescale;
+  d.clk_period = clk_period;
+  gtp_events ev{};
+  return Engine<double>(d, ev, 16).cycleOf(t);
+}
+
+float oracle_n_rise(int prev, int cur) { return nRise(prev, cur); }
+float oracle_n_toggle(int prev, int cur) { return nToggle(prev, cur); }
+
+// Glitch scaling ratio of a pulse of width_ticks ticks on a pin with slews
+// slew_r, slew_f (fp32 = 1: the reference's float arithmetic).
+double oracle_glitch_ratio(int64_t width_ticks, double timescale, float slew_r, float slew_f, int fp32) {
+  gtp_design d{};
+  d.timescale = timescale;
+  d.clk_period = 1e-9f;
+  gtp_events ev{};
+  if (fp32) return static_cast<double>(Engine<float>(d, ev, 16).glitchRatio(width_ticks, slew_r, slew_f));
+  return Engine<double>(d, ev, 16).glitchRatio(width_ticks, slew_r, slew_f);
 }
 
 }  // extern "C"

@@ -38,6 +38,19 @@ def lib() -> C.CDLL:
         L.oracle_n_period.argtypes = [C.c_void_p]
         L.oracle_ticks_per_cycle.restype = C.c_int64
         L.oracle_ticks_per_cycle.argtypes = [C.c_void_p]
+        L.oracle_table_value.restype = C.c_double
+        L.oracle_table_value.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                         C.c_float, C.c_float, C.c_int]
+        L.oracle_find_value_index.restype = C.c_int64
+        L.oracle_find_value_index.argtypes = [C.c_void_p, C.c_int32, C.c_float]
+        L.oracle_cycle_of.restype = C.c_int64
+        L.oracle_cycle_of.argtypes = [C.c_int64, C.c_double, C.c_float]
+        L.oracle_n_rise.restype = C.c_float
+        L.oracle_n_rise.argtypes = [C.c_int, C.c_int]
+        L.oracle_n_toggle.restype = C.c_float
+        L.oracle_n_toggle.argtypes = [C.c_int, C.c_int]
+        L.oracle_glitch_ratio.restype = C.c_double
+        L.oracle_glitch_ratio.argtypes = [C.c_int64, C.c_double, C.c_float, C.c_float, C.c_int]
         _lib = L
     return _lib
 
@@ -99,3 +112,41 @@ def run(design, events, fp32: bool = False, threads: int = 1, cells: np.ndarray 
     if rc != 0:
         raise RuntimeError(f"oracle_run failed: {rc}")
     return OracleResult(cell5, cyc5, tot, grp, ce, cg, ch, cr, ye, yg, int(dropped[0]), secs.value)
+
+
+# ---- the reference's own helpers compiled from its sources (oracle/_ref) ----
+
+REF_LIB = os.path.join(HERE, "_ref", "libref.so")
+_ref = None
+
+
+def build_ref(ref_root: str) -> str:
+    """Compiles the reference helpers (Makefile target `ref`) from the
+    reference sources under ref_root into oracle/_ref/libref.so."""
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    return REF_LIB
+
+
+def ref_lib() -> C.CDLL | None:
+    """The compiled reference helpers, or None when they were not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            return None
+        L = C.CDLL(REF_LIB, mode=os.RTLD_LAZY | os.RTLD_LOCAL)
+        L.ref_table1.restype = C.c_float
+        L.ref_table1.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_float]
+        L.ref_table2.restype = C.c_float
+        L.ref_table2.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_float, C.c_float]
+        L.ref_find_value_index.restype = C.c_longlong
+        L.ref_find_value_index.argtypes = [C.c_void_p, C.c_int, C.c_float]
+        L.ref_clked_waveform_idx.restype = C.c_longlong
+        L.ref_clked_waveform_idx.argtypes = [C.c_longlong, C.c_float, C.c_float]
+        L.ref_n_rise.restype = C.c_float
+        L.ref_n_rise.argtypes = [C.c_int, C.c_int]
+        L.ref_n_toggle.restype = C.c_float
+        L.ref_n_toggle.argtypes = [C.c_int, C.c_int]
+        L.ref_glitch_ratio.restype = C.c_float
+        L.ref_glitch_ratio.argtypes = [C.c_float, C.c_float]
+        _ref = L
+    return _ref

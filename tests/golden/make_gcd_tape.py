@@ -75,7 +75,9 @@ def build(ref_root: str):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_gcd_tape.py <path of the reference checkout>")
+    ref_root = sys.argv[1]
     d, ev, meta = build(ref_root)
     tape.save(os.path.join(HERE, "gcd_tape.npz"), d, ev, meta)
     from oracle import oracle as orc
