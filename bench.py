@@ -65,6 +65,9 @@ def parse():
                          "(with their context), so that each window's copy overlaps the previous walk")
     ap.add_argument("--gates-per-block", type=int, default=0)
     ap.add_argument("--threads-per-block", type=int, default=0)
+    ap.add_argument("--split-events", type=int, default=0,
+                    help="density split: events per thread and tile above which a cell is walked by "
+                         "several threads (0: the engine's default, -1: off)")
     ap.add_argument("--no-clock-runs", action="store_true",
                     help="walk periodic clock pins edge by edge instead of as runs of whole cycles")
     ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream"],
@@ -286,10 +289,11 @@ def run_stream(args):
     del w0
     log(f"autotuner: {best}")
     # device-resident windows, timed walk
-    eng = B200Power(design, **best.engine_kw())
+    eng = B200Power(design, split_events=args.split_events, **best.engine_kw())
     s = torch.cuda.ExternalStream(eng.stream)
     st = synth.DeviceStream(synth.Trace(design, info, spec, seed=20261203 + 2), W)
     total_ev, walk_s, gen_s, n_win, max_win = 0, 0.0, 0.0, 0, 0
+    split_items = []
     host_wins, host_bytes = [], 0
     walk_times = []
     sampler = ClockSampler(0)
@@ -308,6 +312,7 @@ def run_stream(args):
         eng.sync()
         walk_s += a.elapsed_time(b) / 1e3
         walk_times.append(a.elapsed_time(b) / 1e3)
+        split_items.append(eng.walk_items())
         total_ev += w.n_event
         max_win = max(max_win, w.n_event)
         n_win += 1
@@ -325,7 +330,7 @@ def run_stream(args):
     # e2e: host windows through gtp_push_events (double-buffered copies)
     from gtpower_b200.design import Events
     h2d_gbs = h2d_peak_gbs()
-    eng = B200Power(design, **best.engine_kw())
+    eng = B200Power(design, split_events=args.split_events, **best.engine_kw())
     s = torch.cuda.ExternalStream(eng.stream)
     evs = [Events(no.numpy(), tm.numpy(), pk.numpy().view(np.uint32), net_base=nb.numpy(), t_lo=lo, t_hi=hi)
            for (n, lo, hi, no, tm, pk, nb) in host_wins]
@@ -352,7 +357,10 @@ def run_stream(args):
                                f"windows of {W} cycles generated on the GPU",
                    "n_event": total_ev, "windows": n_win, "max_window_events": max_win,
                    "max_window_gb": max_win * 8.25 / 1e9, "autotuned_shape": best.__dict__,
-                   "design_build_s": build_s, "generation_s": gen_s},
+                   "design_build_s": build_s, "generation_s": gen_s,
+                   "density_split": {"split_events": args.split_events,
+                                     "walk_threads_per_tile_max": max(split_items) if split_items else 0,
+                                     "cells": design.n_cell}},
         "e2e": {"value": e2e_ev / e2e_s, "unit": "events/s", "windows": len(host_wins),
                 "same_windows_device_resident_events_per_s": e2e_ev / max(1e-12, sum(walk_times[:len(host_wins)])),
                 "h2d_bytes_per_step": int(host_bytes / max(1, len(host_wins))), "d2h_bytes_per_step": 0,
@@ -710,7 +718,7 @@ def main():
 
     eng = B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                     gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
-                    clock_runs=not args.no_clock_runs)
+                    clock_runs=not args.no_clock_runs, split_events=args.split_events)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     def device_step():
@@ -798,7 +806,8 @@ def main():
     if rank == 0 and not args.no_parity:
         with B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                        gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
-                       clock_runs=not args.no_clock_runs, collect_counts=True) as ceng:
+                       clock_runs=not args.no_clock_runs, split_events=args.split_events,
+                       collect_counts=True) as ceng:
             ceng.push_device(n_event, d_off.data_ptr(), d_t.data_ptr(), d_v.data_ptr())
             counts_res = ceng.fetch(counts=True)
 

@@ -85,7 +85,8 @@ class gtp_config(C.Structure):
                 ("n_thread_per_block", C.c_int32), ("gates_per_block", C.c_int32),
                 ("max_n_pin_for_leakage_power", C.c_int32), ("collect_counts", C.c_int32),
                 ("max_event_num", C.c_int64), ("sort_by_work", C.c_int32),
-                ("clock_runs", C.c_int32), ("reserved", C.c_int64 * 3)]
+                ("clock_runs", C.c_int32), ("split_events", C.c_int32), ("reserved32", C.c_int32),
+                ("reserved", C.c_int64 * 2)]
 
 
 class gtp_counts(C.Structure):
@@ -120,6 +121,8 @@ EXPORTED = sorted([
     "gtp_sync", "gtp_get_stream", "gtp_set_stream", "gtp_finalize", "gtp_fetch",
     "gtp_evaluate_noalloc", "gtp_pack_values",
     "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups", "gtp_clock_run_nets",
+    "gtp_walk_items", "gtp_set_cell_range", "gtp_accumulator_bytes", "gtp_export_accumulators",
+    "gtp_import_accumulators", "gtp_write_cell_power", "gtp_write_per_cycle_waveform",
     "gtp_batch_config_default", "gtp_batch_create", "gtp_batch_destroy", "gtp_batch_last_error",
     "gtp_batch_push_device", "gtp_batch_sync", "gtp_batch_get_stream", "gtp_batch_stats",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
@@ -186,6 +189,20 @@ def lib() -> C.CDLL:
     L.gtp_fetch_cycle_groups.restype = C.c_int32
     L.gtp_clock_run_nets.argtypes = [C.c_void_p, _P, _P]
     L.gtp_clock_run_nets.restype = C.c_int32
+    L.gtp_walk_items.argtypes = [C.c_void_p, _P]
+    L.gtp_walk_items.restype = C.c_int32
+    L.gtp_set_cell_range.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    L.gtp_set_cell_range.restype = C.c_int32
+    L.gtp_accumulator_bytes.argtypes = [C.c_void_p]
+    L.gtp_accumulator_bytes.restype = C.c_int64
+    L.gtp_export_accumulators.argtypes = [C.c_void_p, _P]
+    L.gtp_export_accumulators.restype = C.c_int32
+    L.gtp_import_accumulators.argtypes = [C.c_void_p, _P]
+    L.gtp_import_accumulators.restype = C.c_int32
+    L.gtp_write_cell_power.argtypes = [C.c_char_p, C.c_int32, _P, _P, _P, _P, C.c_char_p]
+    L.gtp_write_cell_power.restype = C.c_int32
+    L.gtp_write_per_cycle_waveform.argtypes = [C.c_char_p, C.c_int64, _P, C.c_char_p, C.c_char_p]
+    L.gtp_write_per_cycle_waveform.restype = C.c_int32
     _bind_proxy(L)
     _lib = L
     return L

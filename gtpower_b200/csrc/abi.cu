@@ -46,6 +46,10 @@ struct gtp_ctx {
   int32_t* d_order_work = nullptr;
   void* d_sort_temp = nullptr;
   size_t sort_temp_bytes = 0;
+  // per-window density split of the walk order (split_events)
+  int32_t* d_item_off = nullptr;
+  void* d_split_temp = nullptr;
+  size_t split_temp_bytes = 0;
   // events (host-pushed windows)
   // events pushed from host memory: two device slots, filled on copy_stream
   // while the walk of the other slot's window runs on `stream`
@@ -124,7 +128,7 @@ void free_all(gtp_ctx* c) {
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
-                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk};
+                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& sl : c->slot)
@@ -292,7 +296,7 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     if (e == cudaSuccess && k.pclk) e = launch_pclk(k, nullptr, c->d_clk_nets, c->n_clk_nets, c->d_pclk, stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tile index");
     if (c->cfg.sort_by_work && c->d_order_work) {
-      e = sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
+      e = sort_cells_by_work(k, c->d_order, P.bucket_begin[3], P.bucket_begin, c->d_keys_in, c->d_keys_out,
                              c->d_order_work, c->d_sort_temp, c->sort_temp_bytes, stream);
       if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
     }
@@ -318,7 +322,7 @@ cudaError_t enqueue_window_prep(gtp_ctx* c, const KParams& k, const KParams* d_k
   }
   if (!(c->cfg.sort_by_work && c->d_order_work)) return cudaSuccess;
   const Packed& P = c->P;
-  return sort_cells_by_work(k, c->d_order, P.n_cell, P.bucket_begin, c->d_keys_in, c->d_keys_out,
+  return sort_cells_by_work(k, c->d_order, P.bucket_begin[3], P.bucket_begin, c->d_keys_in, c->d_keys_out,
                             c->d_order_work, c->d_sort_temp, c->sort_temp_bytes, stream);
 }
 
@@ -336,6 +340,17 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   const Packed& P = c->P;
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   const bool counts = c->cfg.collect_counts != 0;
+  // density split: cells whose measured events per tile exceed split_events
+  // are walked by several threads, each over part of the tile's cycles
+  if (c->d_item_off && c->cfg.sort_by_work && c->d_order_work && P.bucket_begin[3] > 0) {
+    const int32_t se = c->cfg.split_events > 0 ? c->cfg.split_events : kDefaultSplitEvents;
+    const int64_t last_tick = std::min<int64_t>(k.t_hi - 1, k.tmax);
+    const int64_t n_cyc = std::max<int64_t>(1, last_tick / k.tpc + 1 - k.cyc0);
+    cudaError_t e = compute_split(c->d_keys_out, P.bucket_begin[3], k.cycles_per_tile, n_cyc, se, c->d_item_off,
+                                  c->d_split_temp, c->split_temp_bytes, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "density split");
+    k.item_off = c->d_item_off;
+  }
   static const int bucket_pins[3] = {4, 8, kMaxPins};
   for (int b = 0; b < 3; ++b) {
     k.order_begin = P.bucket_begin[b];
@@ -468,6 +483,11 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
       if (e == cudaSuccess) e = cudaMalloc(&c->d_keys_out, sizeof(unsigned long long) * nc);
       if (e == cudaSuccess) e = cudaMalloc(&c->d_order_work, sizeof(int32_t) * nc);
       if (e == cudaSuccess) e = cudaMalloc(&c->d_sort_temp, c->sort_temp_bytes);
+      if (e == cudaSuccess && c->cfg.split_events >= 0) {
+        c->split_temp_bytes = split_temp_bytes(P.n_cell);
+        e = cudaMalloc(&c->d_item_off, sizeof(int32_t) * (nc + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&c->d_split_temp, c->split_temp_bytes);
+      }
     }
     if (e != cudaSuccess) goto cuda_err;
   }
@@ -716,8 +736,9 @@ gtp_status gtp_set_cycle_groups(gtp_ctx* c, const int32_t* cell_group, int32_t n
       std::stable_sort(order.begin() + P.bucket_begin[b], order.begin() + P.bucket_begin[b + 1],
                        [&](int32_t x, int32_t y) { return cell_group[x] < cell_group[y]; });
   }
-  if (nc > 0) {
-    e = cudaMemcpyAsync(c->d_order, order.data(), sizeof(int32_t) * nc, cudaMemcpyHostToDevice, c->stream);
+  if (!order.empty()) {
+    e = cudaMemcpyAsync(c->d_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice,
+                        c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "walk order upload");
   }
@@ -749,6 +770,86 @@ gtp_status gtp_set_cycle_groups(gtp_ctx* c, const int32_t* cell_group, int32_t n
 
 int32_t gtp_n_cycle_groups(const gtp_ctx* c) { return c ? c->n_cgroup : 0; }
 
+gtp_status gtp_set_cell_range(gtp_ctx* c, int32_t cell_begin, int32_t cell_end) {
+  if (!c) return GTP_EINVAL;
+  Packed& P = c->P;
+  if (c->any_window || c->n_cgroup > 0) {
+    c->err = "gtp_set_cell_range: call before the first window (or after gtp_reset) and before "
+             "gtp_set_cycle_groups";
+    return GTP_ESTATE;
+  }
+  if (cell_begin < 0 || cell_end < cell_begin || cell_end > P.n_cell) {
+    c->err = "gtp_set_cell_range: need 0 <= cell_begin <= cell_end <= n_cell";
+    return GTP_EINVAL;
+  }
+  // the whole design's walk order, keeping the cells of the range (bucket
+  // grouping and type order stay as packed)
+  std::vector<int32_t> order;
+  order.reserve(static_cast<size_t>(cell_end - cell_begin));
+  int32_t bb[4] = {0, 0, 0, 0};
+  for (int b = 0; b < 3; ++b) {
+    bb[b] = static_cast<int32_t>(order.size());
+    for (int32_t i = P.bucket_all[b]; i < P.bucket_all[b + 1]; ++i)
+      if (P.order_all[i] >= cell_begin && P.order_all[i] < cell_end) order.push_back(P.order_all[i]);
+  }
+  bb[3] = static_cast<int32_t>(order.size());
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess && !order.empty())
+    e = cudaMemcpyAsync(c->d_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "gtp_set_cell_range");
+  P.order.swap(order);
+  for (int b = 0; b < 4; ++b) P.bucket_begin[b] = bb[b];
+  return GTP_OK;
+}
+
+int64_t gtp_accumulator_bytes(const gtp_ctx* c) {
+  if (!c) return -1;
+  const int64_t nc = c->P.n_cell, ny = c->P.n_period + 1;
+  int64_t b = 8 * kNumCellAcc * nc + 8 * kNumCycAcc * ny;
+  if (c->cfg.collect_counts) b += 8 * 2 * ny + 4 * 4 * nc;
+  return b;
+}
+
+// Accumulator block layout (gtp_accumulator_bytes): FP64 cell sums
+// [5][n_cell] | int64 per-cycle fixed-point bins [6][n_period+1] | with
+// collect_counts: uint64 per-cycle counts [2][n_period+1] | uint32 per-cell
+// counts [4][n_cell].
+namespace {
+gtp_status copy_accumulators(gtp_ctx* c, void* dst, const void* src, bool out) {
+  if (!c || !dst || !src) return GTP_EINVAL;
+  const size_t nc = static_cast<size_t>(c->P.n_cell), ny = static_cast<size_t>(c->P.n_period + 1);
+  struct Seg {
+    void* dev;
+    size_t bytes;
+  } segs[4] = {{c->d_cell_acc, 8 * kNumCellAcc * nc},
+               {c->d_cyc_acc, 8 * kNumCycAcc * ny},
+               {c->d_cnt_cyc, c->cfg.collect_counts ? 8 * 2 * ny : 0},
+               {c->d_cnt_cell, c->cfg.collect_counts ? 4 * 4 * nc : 0}};
+  size_t off = 0;
+  for (const Seg& sg : segs) {
+    if (sg.bytes == 0) continue;
+    cudaError_t e =
+        out ? cudaMemcpyAsync(static_cast<char*>(dst) + off, sg.dev, sg.bytes, cudaMemcpyDeviceToDevice, c->stream)
+            : cudaMemcpyAsync(sg.dev, static_cast<const char*>(src) + off, sg.bytes, cudaMemcpyDeviceToDevice,
+                              c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, out ? "gtp_export_accumulators" : "gtp_import_accumulators");
+    off += sg.bytes;
+  }
+  return GTP_OK;
+}
+}  // namespace
+
+gtp_status gtp_export_accumulators(gtp_ctx* c, void* d_out) {
+  return copy_accumulators(c, d_out, c ? c->d_cell_acc : nullptr, true);
+}
+
+gtp_status gtp_import_accumulators(gtp_ctx* c, const void* d_in) {
+  gtp_status st = copy_accumulators(c, c ? c->d_cell_acc : nullptr, d_in, false);
+  if (st == GTP_OK) c->any_window = true;
+  return st;
+}
+
 gtp_status gtp_clock_run_nets(gtp_ctx* c, int32_t* n_clock_nets, int32_t* n_periodic) {
   if (!c || !n_clock_nets || !n_periodic) return GTP_EINVAL;
   *n_clock_nets = c->n_clk_nets;
@@ -762,6 +863,20 @@ gtp_status gtp_clock_run_nets(gtp_ctx* c, int32_t* n_clock_nets, int32_t* n_peri
   for (int32_t net : c->clk_nets)
     if (tab[static_cast<size_t>(net)].x >= 0) ++n;
   *n_periodic = n;
+  return GTP_OK;
+}
+
+gtp_status gtp_walk_items(gtp_ctx* c, int64_t* items) {
+  if (!c || !items) return GTP_EINVAL;
+  *items = 0;
+  const int32_t n_order = c->P.bucket_begin[3];
+  if (!c->d_item_off || n_order <= 0 || !c->any_window) return GTP_OK;
+  int32_t n = 0;
+  cudaError_t e = cudaMemcpyAsync(&n, c->d_item_off + n_order, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "walk items");
+  *items = n;
   return GTP_OK;
 }
 

@@ -100,8 +100,12 @@ struct Packed {
   // leakage split departs from the plain overlap (needs the drift path)
   bool drift = false;
   int32_t fast_inst_floats = 0;   // largest instance block of a fast cell type
-  // bucket ranges in order[]: cells with n_pin <= 4, <= 8, <= 32
+  // bucket ranges in order[]: cells with n_pin <= 4, <= 8, <= 32; order[]
+  // lists the cells the context walks (all, or a shard, gtp_set_cell_range),
+  // bucket_begin[3] of them; order_all / bucket_all: the whole design's
+  std::vector<int32_t> order_all;
   int32_t bucket_begin[4] = {0, 0, 0, 0};
+  int32_t bucket_all[4] = {0, 0, 0, 0};
   double max_abs_energy = 0;     // max |instance energy|, for the fixed-point scale
   double max_abs_leak = 0;
 };
@@ -183,6 +187,11 @@ struct KParams {
   const int32_t* cell_cgroup;       // [n_cell] group of each cell, or null
   int32_t n_cgroup;
   unsigned long long* cyc_acc_g;    // [n_cgroup][6][n_period+1]
+  // density split (optional, one-window walk only): item_off[k] = first walk
+  // item of the cell at walk-order position k (exclusive prefix over
+  // positions of the number of threads that walk it per tile), n_cell + 1
+  // entries; null = one thread per cell and tile
+  const int32_t* item_off;
 };
 
 // status bits set by the kernel
@@ -250,6 +259,26 @@ cudaError_t sort_cells_by_work(const KParams& p, const int32_t* base_order, int3
                                const int32_t* bucket_begin, unsigned long long* keys_in,
                                unsigned long long* keys_out, int32_t* order_out, void* temp,
                                size_t temp_bytes, cudaStream_t stream);
+
+// Most threads one cell is split into per tile by the density rule.
+constexpr int32_t kMaxSplit = 32;
+// Default events per thread and tile above which a cell is split.
+constexpr int32_t kDefaultSplitEvents = 2048;
+
+// Density split of one window, after sort_cells_by_work (keys_sorted: the
+// sorted keys, whose low 39 bits hold the inverted event count of the cell
+// at each walk-order position): the cell at position k is walked by
+// n_k = clamp(ceil(work_k * cycles_per_tile / n_cyc / split_events), 1,
+// min(kMaxSplit, cycles_per_tile)) threads per tile, each over 1/n_k of the
+// tile's cycles; item_off (n_cell + 1 entries) receives the exclusive prefix
+// of n_k. n_cyc: cycles of the window. temp: split_temp_bytes(n_cell) bytes.
+size_t split_scan_temp_bytes(int32_t n_cell);
+inline size_t split_temp_bytes(int32_t n_cell) {
+  return ((static_cast<size_t>(n_cell) + 1) * 4 + 255) / 256 * 256 + split_scan_temp_bytes(n_cell);
+}
+cudaError_t compute_split(const unsigned long long* keys_sorted, int32_t n_cell, int64_t cycles_per_tile,
+                          int64_t n_cyc, int32_t split_events, int32_t* item_off, void* temp, size_t temp_bytes,
+                          cudaStream_t stream);
 
 // Finalize kernels: per-cell floats, totals/groups, per-cycle floats.
 // With d_cycle5_g (and p.cyc_acc_g), also the per-group per-cycle floats

@@ -424,6 +424,8 @@ gtp_status pack_design(const gtp_design& d, int max_leak_pins, Packed& P, std::s
     while (i < d.n_cell && bucket(P.order[i]) < b) ++i;
     P.bucket_begin[b] = i;
   }
+  P.order_all = P.order;
+  for (int b = 0; b < 4; ++b) P.bucket_all[b] = P.bucket_begin[b];
   return GTP_OK;
 }
 

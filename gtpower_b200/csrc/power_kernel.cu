@@ -30,6 +30,7 @@
 // 32-bit offsets from the tile start.
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
 #include "engine.h"
@@ -311,7 +312,7 @@ __device__ __forceinline__ float glitch_ratio(const KParams& p, int64_t e, int64
 // of one pin bucket over cycle tile `tile` of the window, with the block's
 // dynamic shared memory `smem`. All threads of the block call it together.
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS, bool RING_EV>
-__device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile,
+__device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile, const int n_blk,
                                            unsigned long long* smem) {
   const int64_t ct = p.cycles_per_tile;
   // per-cycle groups: two bin sets, for the block's first group and the next
@@ -381,14 +382,53 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     r_exist = static_cast<int32_t>(max(tl, -static_cast<int64_t>(INT32_MAX / 2)));
   }
 
-  const int32_t g_begin = p.order_begin + gblk * p.gates_per_block;
-  const int32_t g_end = min(p.order_end, g_begin + p.gates_per_block);
+  // The block's work: without a split table, the cells order[g_begin, g_end)
+  // of the bucket (one thread each); with one (density split), walk items
+  // of the bucket's item space [ib0, ie0) in chunks of gates_per_block:
+  // chunk gblk, then gblk + n_blk, ... while items remain. Item it is
+  // sub-walk it - item_off[k] of the cell at walk-order position k.
+  const bool split = p.item_off != nullptr;
+  const int32_t ib0 = split ? __ldg(p.item_off + p.order_begin) : p.order_begin;
+  const int32_t ie0 = split ? __ldg(p.item_off + p.order_end) : p.order_end;
+  // walk-order position of item it: the last k in [order_begin, order_end)
+  // with item_off[k] <= it
+  auto pos_of = [&](int32_t it) -> int32_t {
+    if (!split) return it;
+    int32_t lo = p.order_begin, hi = p.order_end;   // item_off[lo] <= it < item_off[hi]
+    while (hi - lo > 1) {
+      const int32_t m = lo + ((hi - lo) >> 1);
+      if (__ldg(p.item_off + m) <= it) lo = m; else hi = m;
+    }
+    return lo;
+  };
+  const int64_t first_item = static_cast<int64_t>(ib0) + static_cast<int64_t>(gblk) * p.gates_per_block;
   // cells are ordered by group within a bucket: the block's first cell has
   // its smallest group
-  const int32_t g_first = p.cell_cgroup ? __ldg(p.cell_cgroup + __ldg(p.order + g_begin)) : 0;
+  const int32_t g_first = (p.cell_cgroup && first_item < ie0)
+                              ? __ldg(p.cell_cgroup + __ldg(p.order + pos_of(static_cast<int32_t>(first_item))))
+                              : 0;
 
-  for (int32_t gi = g_begin + threadIdx.x; gi < g_end; gi += blockDim.x) {
+  for (int64_t chunk = gblk;; chunk += n_blk) {
+  const int64_t cb = static_cast<int64_t>(ib0) + chunk * p.gates_per_block;
+  if (cb >= ie0) break;
+  const int32_t ce = static_cast<int32_t>(min(static_cast<int64_t>(ie0), cb + p.gates_per_block));
+  for (int32_t it = static_cast<int32_t>(cb) + threadIdx.x; it < ce; it += blockDim.x) {
+    const int32_t gi = pos_of(it);
+    const int32_t sub = split ? it - __ldg(p.item_off + gi) : 0;
+    const int32_t nsub = split ? __ldg(p.item_off + gi + 1) - __ldg(p.item_off + gi) : 1;
     const int32_t cell = __ldg(p.order + gi);
+    // this thread's part of the tile: ticks [T0 + s0r, T0 + s1r), the
+    // cycles [sub * ct / nsub, (sub + 1) * ct / nsub) of the tile
+    uint32_t s0r = 0, s1r = span;
+    if (nsub > 1) {
+      auto bnd = [&](int64_t k) -> uint32_t {
+        const int64_t r = k * static_cast<int64_t>(tpc32) - static_cast<int64_t>(off0);
+        return r <= 0 ? 0u : (r >= static_cast<int64_t>(span) ? span : static_cast<uint32_t>(r));
+      };
+      s0r = bnd(static_cast<int64_t>(sub) * ct / nsub);
+      if (sub + 1 < nsub) s1r = bnd(static_cast<int64_t>(sub + 1) * ct / nsub);
+    }
+    const bool owns_initial_cell = owns_initial && sub == 0;
     if (p.cell_cgroup) {
       bins.g = __ldg(p.cell_cgroup + cell);
       const int32_t set = bins.g - g_first;
@@ -457,7 +497,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     };
     auto rel = [&](int64_t t) -> uint32_t {
       const int64_t r = t - T0;
-      return (r >= 0 && r < static_cast<int64_t>(span)) ? static_cast<uint32_t>(r) : kRelBeyond;
+      return (r >= 0 && r < static_cast<int64_t>(s1r)) ? static_cast<uint32_t>(r) : kRelBeyond;
     };
     // RING: read up to kRing events of pin i into its buffer with
     // independent loads (one memory latency per kRing events)
@@ -528,15 +568,16 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
           } else if (e > a) {
             has_wave |= 1u << i;
             const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
-            // lower_bound(T0) in [a, e): from the window's per-(tile, net)
-            // index when it was built, else by bisection
+            // lower_bound(T0 + s0r) in [a, e): the tile's start from the
+            // window's per-(tile, net) index when it was built, then (or
+            // else) by bisection
             int64_t l = a, r = e;
-            if (p.tile_first) {
-              l = a + __ldg(p.tile_first + static_cast<int64_t>(tile) * p.n_net + net);
-            } else {
+            const int64_t S0 = T0 + static_cast<int64_t>(s0r);
+            if (p.tile_first) l = a + __ldg(p.tile_first + static_cast<int64_t>(tile) * p.n_net + net);
+            if (!p.tile_first || s0r > 0) {
               while (l < r) {
                 const int64_t m = l + ((r - l) >> 1);
-                if (ev_time(p.ev_t, m) < T0) l = m + 1; else r = m;
+                if (ev_time(p.ev_t, m) < S0) l = m + 1; else r = m;
               }
             }
             // the waveform's first event at tick 0 is the initial condition
@@ -604,7 +645,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     // end of the tile's edges: those before span, or before time_max when the
     // edge there is absent
     auto pclk_jend = [&]() -> uint32_t {
-      const int64_t r_end = ((pBv >> 30) & 1u) ? min(static_cast<int64_t>(span), p.tmax - T0) : static_cast<int64_t>(span);
+      const int64_t r_end = ((pBv >> 30) & 1u) ? min(static_cast<int64_t>(s1r), p.tmax - T0) : static_cast<int64_t>(s1r);
       if (r_end <= 0) return 0u;
       const uint32_t ce = udiv32(static_cast<uint32_t>(r_end - 1) + off0, tpc32, p.tpc_magic);
       const int32_t he = static_cast<int32_t>(static_cast<uint32_t>(r_end - 1) + off0 - ce * tpc32);
@@ -674,11 +715,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       }
     };
     if (pkbit) {
-      // first edge at or after max(0, r_exist)
-      const uint32_t ph0 = off0 + static_cast<uint32_t>(max(0, r_exist));
-      pj = ph0 <= pA ? 0u : (ph0 <= pB ? 1u : 2u);
+      // first edge at or after max(s0r, r_exist)
+      const uint32_t ph0 = off0 + static_cast<uint32_t>(max(static_cast<int32_t>(s0r), r_exist));
+      const uint32_t q0 = udiv32(ph0, tpc32, p.tpc_magic);
+      const uint32_t h0 = ph0 - q0 * tpc32;
+      pj = 2 * q0 + (h0 > pA ? 1u : 0u) + (h0 > pB ? 1u : 0u);
     }
-    if (owns_initial) {
+    if (owns_initial_cell) {
       acc_add(4, static_cast<double>(leak_cur) * static_cast<double>(p.tmax));
       add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak_cur) * P, p.fx_leak));
     }
@@ -706,7 +749,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 #pragma unroll
       for (int i = 0; i < MAXP; ++i)
         if (i < n_pin) cur = min(cur, nt[i]);
-      if (cur >= span) break;
+      if (cur >= s1r) break;
       const int64_t cur_abs = T0 + cur;
       const uint32_t cq = udiv32(cur + off0, tpc32, p.tpc_magic);     // cycles after c_lo
       const int64_t cyc = bins.c_lo + cq;
@@ -978,6 +1021,8 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       if (n_rel) atomicAdd(p.cnt_cell + 3 * nc + cell, n_rel);
     }
   }
+  if (!split) break;
+  }
 
   __syncthreads();
   // clock runs: run-differences -> per-cycle sums
@@ -1019,7 +1064,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
   extern __shared__ unsigned long long smem[];
-  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, smem);
+  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, gridDim.x, smem);
 }
 
 // Persistent walk over the windows of many designs: each block takes work
@@ -1045,7 +1090,7 @@ __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS)
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sp);
     for (int k = threadIdx.x; k < static_cast<int>(sizeof(KParams) / 8); k += blockDim.x) dst[k] = src[k];
     __syncthreads();
-    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_BATCH_RING>(sp, w.y, w.z, smem);
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_BATCH_RING>(sp, w.y, w.z, 1, smem);
     __syncthreads();  // smem and s_item are reused by the next item
   }
 }
@@ -1288,7 +1333,53 @@ __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ ba
     keys[k] = (bucket << 40) | cls | (cap - wc);
 }
 
+// ---- density split ----
+
+// cnt[k] = threads that walk the cell at walk-order position k per tile
+// (cnt[n] = 0, the end of the prefix): the events the cell's pins list in
+// the window, spread over one tile at the window's mean density, per
+// split_events events, within [1, min(kMaxSplit, ct)].
+__global__ void split_count_kernel(const unsigned long long* __restrict__ keys, int32_t n, int64_t ct,
+                                   int64_t n_cyc, int32_t split_events, int32_t* __restrict__ cnt) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > n) return;
+  if (k == n) {
+    cnt[k] = 0;
+    return;
+  }
+  const unsigned long long cap = (1ull << 39) - 1;
+  const unsigned long long wc = cap - (keys[k] & cap);
+  const double per_tile = static_cast<double>(wc) * static_cast<double>(ct) /
+                          static_cast<double>(n_cyc > 0 ? n_cyc : 1);
+  const int64_t lim = ct < kMaxSplit ? ct : kMaxSplit;
+  int64_t m = static_cast<int64_t>(ceil(per_tile / static_cast<double>(split_events)));
+  m = m < 1 ? 1 : (m > lim ? lim : m);
+  cnt[k] = static_cast<int32_t>(m);
+}
+
 }  // namespace
+
+size_t split_scan_temp_bytes(int32_t n_cell) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
+                                n_cell + 1);
+  return bytes;
+}
+
+cudaError_t compute_split(const unsigned long long* keys_sorted, int32_t n_cell, int64_t cycles_per_tile,
+                          int64_t n_cyc, int32_t split_events, int32_t* item_off, void* temp, size_t temp_bytes,
+                          cudaStream_t stream) {
+  if (n_cell <= 0) return cudaSuccess;
+  // counts first into the temp area's head, then the scan into item_off
+  int32_t* cnt = static_cast<int32_t*>(temp);
+  void* scan_temp = static_cast<char*>(temp) + ((static_cast<size_t>(n_cell) + 1) * 4 + 255) / 256 * 256;
+  size_t scan_bytes = temp_bytes - (static_cast<char*>(scan_temp) - static_cast<char*>(temp));
+  split_count_kernel<<<(n_cell + 1 + 255) / 256, 256, 0, stream>>>(keys_sorted, n_cell, cycles_per_tile, n_cyc,
+                                                                    split_events, cnt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cub::DeviceScan::ExclusiveSum(scan_temp, scan_bytes, cnt, item_off, n_cell + 1, stream);
+}
 
 cudaError_t launch_glitch_pw(const KParams& p, const KParams* d_p, float* out, cudaStream_t stream) {
   if (p.n_net <= 0) return cudaSuccess;

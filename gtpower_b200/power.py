@@ -41,23 +41,25 @@ class PowerResult:
         return self.internal + self.switching + self.leakage
 
     def print_per_cycle_results(self, path: str, top_name: str, sep: str = "\t") -> None:
-        """PowerResult::printPerCycleResults (include/sta/PowerClass.hh:123-149)."""
-        titles = ["Per cycle leakage power: ", "Per cycle internal power: ",
-                  "Per cycle glitch internal power: ", "Per cycle switching power: ",
-                  "Per cycle glitch switching power: "]
-        with open(path, "w") as f:
-            for q, t in enumerate(titles):
-                f.write(t + "\n")
-                if self.waveforms is not None:
-                    f.write(top_name + sep)
-                    f.write("".join(_fmt6(float(v)) + sep for v in self.waveforms[q]))
-                    f.write("\n")
-            f.write("End of per cycle power\n")
+        """PowerResult::printPerCycleResults (include/sta/PowerClass.hh:123-149),
+        written by the library (gtp_write_per_cycle_waveform)."""
+        w = np.ascontiguousarray(self.waveforms if self.waveforms is not None else np.zeros((5, 0)),
+                                 dtype=np.float32)
+        _abi.check(_abi.lib().gtp_write_per_cycle_waveform(path.encode(), int(w.shape[1]),
+                                                           w.ctypes.data_as(C.c_void_p), top_name.encode(),
+                                                           sep.encode()))
 
 
-def _fmt6(v: float) -> str:
-    """std::ostream default formatting of a float (%g, 6 significant digits)."""
-    return f"{v:g}"
+def write_cell_power(path: str, design: Design, cell5: np.ndarray, sep: str = "\t") -> None:
+    """cuda_cell_power.txt from per-cell results [n_cell, 5] (gtp_write_cell_power)."""
+    names = design.cell_names or [f"inst{i}" for i in range(design.n_cell)]
+    c_names = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+    t_names = (C.c_char_p * max(1, len(design.lib.names)))(*[n.encode() for n in design.lib.names])
+    c5 = np.ascontiguousarray(cell5, dtype=np.float32)
+    ct = np.ascontiguousarray(design.cell_type, dtype=np.int32)
+    _abi.check(_abi.lib().gtp_write_cell_power(path.encode(), design.n_cell, c5.ctypes.data_as(C.c_void_p),
+                                               C.cast(c_names, C.c_void_p), ct.ctypes.data_as(C.c_void_p),
+                                               C.cast(t_names, C.c_void_p), sep.encode()))
 
 
 @dataclass
@@ -86,7 +88,7 @@ class B200Power:
     def __init__(self, design: Design, *, collect_counts: bool = False, device: int = -1,
                  cycles_per_tile: int = 0, threads_per_block: int = 0, gates_per_block: int = 0,
                  max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None,
-                 clock_runs: bool = True):
+                 clock_runs: bool = True, split_events: int = 0):
         self.design = design
         L = _abi.lib()
         cfg = _abi.gtp_config()
@@ -101,6 +103,9 @@ class B200Power:
             cfg.sort_by_work = 1 if sort_by_work else 0
         # periodic clock pins walked as runs of whole cycles (False: edge by edge)
         cfg.clock_runs = 1 if clock_runs else -1
+        # density split: events per thread and tile above which a cell's tile
+        # is shared by several threads (0: the default 2048, -1: off)
+        cfg.split_events = split_events
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()
@@ -180,6 +185,13 @@ class B200Power:
         _abi.check(_abi.lib().gtp_clock_run_nets(self.ctx, C.byref(n_clk), C.byref(n_per)), self.ctx)
         return int(n_clk.value), int(n_per.value)
 
+    def walk_items(self) -> int:
+        """Threads per tile that walked the last one-window push (n_cell when
+        the density split split no cell, 0 when the split is off)."""
+        n = C.c_int64(0)
+        _abi.check(_abi.lib().gtp_walk_items(self.ctx, C.byref(n)), self.ctx)
+        return int(n.value)
+
     def fetch_cycle_groups(self) -> np.ndarray:
         """[n_group, 5, n_period] float32: the cycle5 rows of each group."""
         L = _abi.lib()
@@ -232,21 +244,10 @@ class B200Power:
         return total, seq, comb, clock, macro, pad
 
     def print_cell_res(self, path: str, sep: str = "\t") -> None:
-        """CudaPower::printCellRes (power/cuda/CudaPower.cu:3134-3165)."""
+        """CudaPower::printCellRes (power/cuda/CudaPower.cu:3134-3165), written
+        by the library (gtp_write_cell_power)."""
         r = self._results or self.fetch()
-        d = self.design
-        names = d.cell_names or [f"inst{i}" for i in range(d.n_cell)]
-        with open(path, "w") as f:
-            f.write(sep.join(["cell", "Internal_Power", "Glitch_Internal_Power", "Switching_Power",
-                              "Glitch_Switching_Power", "Leakage_Power", "Total_Power",
-                              "Standard_Cell"]) + "\n")
-            c5 = r.cell5
-            for i in range(d.n_cell):
-                v = c5[i]
-                tot = np.float32(np.float32(np.float32(np.float32(v[0] + v[1]) + v[2]) + v[3]) + v[4])
-                cell_name = d.lib.names[d.cell_type[i]]
-                f.write(sep.join([names[i]] + [_fmt6(float(x)) for x in v] +
-                                 [_fmt6(float(tot)), cell_name]) + "\n")
+        write_cell_power(path, self.design, r.cell5, sep)
 
     def report_power(self, digits: int = 3) -> str:
         """The report_power group table (power/Power.tcl:68-90)."""

@@ -210,7 +210,20 @@ typedef struct gtp_config {
                                         fixed phases) are walked as runs of whole
                                         cycles between the cell's other events:
                                         0 or 1 = on (default), -1 = edge by edge */
-  int64_t reserved[3];
+  int32_t split_events;              /* density-aware split, as the reference's
+                                        cycles-per-thread rule (Gate::
+                                        setNCyclePerThreadByEventCount,
+                                        power/cuda/Gate.cuh:354-376): per window,
+                                        a cell whose measured event density rho
+                                        (its pins' events per cycle, periodic
+                                        clock pins excluded) gives more than
+                                        split_events events in one cycle tile is
+                                        walked by n = ceil(rho * tile /
+                                        split_events) threads (at most 32), each
+                                        over 1/n of the tile's cycles;
+                                        0 = 2048, -1 = off. Needs sort_by_work. */
+  int32_t reserved32;
+  int64_t reserved[2];
 } gtp_config;
 
 /* Integer counters that must match the oracle bit-exactly. */
@@ -302,6 +315,38 @@ gtp_status  gtp_fetch_cycle_groups(gtp_ctx* ctx, float* cycle5_groups);
  * the context's stream. */
 gtp_status  gtp_clock_run_nets(gtp_ctx* ctx, int32_t* n_clock_nets, int32_t* n_periodic);
 
+/* Sharding one design across GPUs. No counterpart in the reference, which
+ * runs on one device (power/cuda/CudaPower.cu:1227-1337).
+ *
+ * Cells are independent given their pins' event lists, so N contexts (one
+ * per GPU, each created from the whole design so that all share one
+ * fixed-point scale) can each walk a contiguous cell range and add their
+ * accumulators. gtp_set_cell_range restricts a context to cells
+ * [cell_begin, cell_end) (call before the first window or after gtp_reset,
+ * and before gtp_set_cycle_groups); its windows need to list only the nets
+ * those cells read (other nets may be empty). gtp_export_accumulators copies
+ * the context's accumulators (gtp_accumulator_bytes bytes, device to device,
+ * on the context's stream) in the layout
+ *   double  cell[5][n_cell]          per-cell energy and leakage sums
+ *   int64   cycle[6][n_period+1]     per-cycle 64-bit fixed-point bins
+ *   uint64  cycle_counts[2][n_period+1]   (with collect_counts)
+ *   uint32  cell_counts[4][n_cell]        (with collect_counts)
+ * Summed over the shards element-wise (FP64 for the cell sums, which are
+ * disjoint, wrap-around integer addition for the rest: exact and
+ * order-independent), the block imported into any shard's context with
+ * gtp_import_accumulators makes gtp_fetch return the whole design's
+ * results. Per-cycle waveforms by cell group are not carried. */
+gtp_status  gtp_set_cell_range(gtp_ctx* ctx, int32_t cell_begin, int32_t cell_end);
+int64_t     gtp_accumulator_bytes(const gtp_ctx* ctx);
+gtp_status  gtp_export_accumulators(gtp_ctx* ctx, void* d_out);
+gtp_status  gtp_import_accumulators(gtp_ctx* ctx, const void* d_in);
+
+/* Density split (gtp_config.split_events); a diagnostic of this engine.
+ * *items = threads per tile that walked the context's last one-window push
+ * (n_cell when no cell was split; n_cell + the extra threads of split cells
+ * otherwise; 0 when the split is off). Waits for the context's stream. */
+gtp_status  gtp_walk_items(gtp_ctx* ctx, int64_t* items);
+
 /* Allocation-free evaluation. No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run, e.g. an
@@ -359,6 +404,31 @@ void*       gtp_batch_get_stream(const gtp_batch* b);
 /* Work items and persistent launches of the last push; graph replays so far. */
 gtp_status  gtp_batch_stats(const gtp_batch* b, int64_t* items, int32_t* launches,
                             int32_t* graph_replays);
+
+/* The reference's result files, from fetched results (host arrays; no
+ * context or device needed), written with the reference's expressions and
+ * std::ostream formatting:
+ *   gtp_write_cell_power: cuda_cell_power.txt (CudaPower::printCellRes,
+ *     power/cuda/CudaPower.cu:3134-3165; the CPU path's cpu_cell_power.txt,
+ *     Power::printCellRes, power/Power.cc:389-422, has the same layout).
+ *     cell5 [n_cell][5] as gtp_fetch; one row per cell in cell index order,
+ *     named cell_names[i], with the Liberty cell name
+ *     type_names[cell_type[i]] (both may be NULL: empty names). The
+ *     internal and switching columns are formed as the reference forms them:
+ *     (regular + glitch) folded in float, then folded - glitch.
+ *   gtp_write_per_cycle_waveform: cuda_per_cycle_waveform.txt
+ *     (PowerResult::printPerCycleResults, include/sta/PowerClass.hh:123-149):
+ *     five sections (leakage, internal, glitch internal, switching, glitch
+ *     switching), each the design total's waveform cycle5 [5][n_period]
+ *     under top_name.
+ * sep: the column separator (NULL: a tab, G_CONFIG's default,
+ * util/GlobalConfig.hh:50). GTP_GENERAL_ERROR when the file cannot be
+ * written. */
+gtp_status  gtp_write_cell_power(const char* path, int32_t n_cell, const float* cell5,
+                                 const char* const* cell_names, const int32_t* cell_type,
+                                 const char* const* type_names, const char* sep);
+gtp_status  gtp_write_per_cycle_waveform(const char* path, int64_t n_period, const float* cycle5,
+                                         const char* top_name, const char* sep);
 
 /* Packs one value per byte (0..3) into the 2-bit layout of value_packed. */
 void        gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed);
