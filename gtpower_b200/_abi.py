@@ -122,7 +122,7 @@ EXPORTED = sorted([
     "gtp_evaluate_noalloc", "gtp_pack_values",
     "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups", "gtp_clock_run_nets",
     "gtp_walk_items", "gtp_set_cell_range", "gtp_accumulator_bytes", "gtp_export_accumulators",
-    "gtp_import_accumulators", "gtp_write_cell_power", "gtp_write_per_cycle_waveform",
+    "gtp_import_accumulators", "gtp_push_events_device_ranges", "gtp_write_cell_power", "gtp_write_per_cycle_waveform",
     "gtp_batch_config_default", "gtp_batch_create", "gtp_batch_destroy", "gtp_batch_last_error",
     "gtp_batch_push_device", "gtp_batch_sync", "gtp_batch_get_stream", "gtp_batch_stats",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
@@ -199,6 +199,8 @@ def lib() -> C.CDLL:
     L.gtp_export_accumulators.restype = C.c_int32
     L.gtp_import_accumulators.argtypes = [C.c_void_p, _P]
     L.gtp_import_accumulators.restype = C.c_int32
+    L.gtp_push_events_device_ranges.argtypes = [C.c_void_p, C.POINTER(gtp_events), _P, C.c_int32]
+    L.gtp_push_events_device_ranges.restype = C.c_int32
     L.gtp_write_cell_power.argtypes = [C.c_char_p, C.c_int32, _P, _P, _P, _P, C.c_char_p]
     L.gtp_write_cell_power.restype = C.c_int32
     L.gtp_write_per_cycle_waveform.argtypes = [C.c_char_p, C.c_int64, _P, C.c_char_p, C.c_char_p]

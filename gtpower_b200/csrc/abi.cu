@@ -46,6 +46,9 @@ struct gtp_ctx {
   int32_t* d_order_work = nullptr;
   void* d_sort_temp = nullptr;
   size_t sort_temp_bytes = 0;
+  // tiles of a cycle-range push
+  int2* d_tiles = nullptr;
+  size_t tiles_cap = 0;
   // per-window density split of the walk order (split_events)
   int32_t* d_item_off = nullptr;
   void* d_split_temp = nullptr;
@@ -128,7 +131,7 @@ void free_all(gtp_ctx* c) {
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
-                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp};
+                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp, c->d_tiles};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& sl : c->slot)
@@ -214,9 +217,12 @@ bool clock_runs_on(const gtp_ctx* c) {
 // Validates one window and sets up its walk parameters *out (sorting the
 // walk order by work on `stream` when configured). The context's window
 // state advances only when the walk is enqueued (commit_window).
+// ranges (pairs of cycles [c0, c1), ascending and disjoint) restrict the
+// walk to those cycles of the window.
 gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t, const uint32_t* d_v,
                           const int64_t* d_base, int64_t n_event, int64_t t_lo, int64_t t_hi,
-                          cudaStream_t stream, KParams* out, bool enqueue_prep = true) {
+                          cudaStream_t stream, KParams* out, bool enqueue_prep = true,
+                          const std::vector<int64_t>* ranges = nullptr) {
   if (t_hi <= t_lo) { c->err = "t_hi must exceed t_lo"; return GTP_EINVAL; }
   if (t_lo < 0) { c->err = "t_lo must be >= 0"; return GTP_EINVAL; }
   if (c->any_window && t_lo < c->last_t_hi) {
@@ -224,6 +230,12 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     return GTP_ESTATE;
   }
   const Packed& P = c->P;
+  // a window that does not continue the last one (a gap, a first window
+  // after tick 0, or cycle ranges) is evaluated on its own: its leakage
+  // starts at its first tick instead of carrying over
+  const bool standalone = ranges != nullptr || (!c->any_window && t_lo > 0) ||
+                          (c->any_window && t_lo > c->last_t_hi);
+
   KParams k = make_params(c);
   k.net_off = d_net_off;
   k.ev_t = d_t;
@@ -254,6 +266,35 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   if (ct > max_ct || ct < 1) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
   k.cycles_per_tile = ct;
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
+  k.standalone = standalone ? 1 : 0;
+  if (ranges) {
+    // tiles of at most ct cycles over the ranges, within the window
+    std::vector<int2> tiles;
+    const int64_t cyc_end_w = k.cyc0 + n_cyc;
+    for (size_t r = 0; r + 1 < ranges->size(); r += 2) {
+      const int64_t c0 = std::max<int64_t>((*ranges)[r], k.cyc0), c1 = std::min<int64_t>((*ranges)[r + 1], cyc_end_w);
+      for (int64_t cc = c0; cc < c1; cc += ct)
+        tiles.push_back(make_int2(static_cast<int>(cc), static_cast<int>(std::min<int64_t>(ct, c1 - cc))));
+    }
+    if (tiles.size() > 65535) { c->err = "cycle ranges need more than 65535 tiles"; return GTP_EOVERFLOW; }
+    if (tiles.size() > c->tiles_cap) {
+      cudaError_t e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "sync");
+      if (c->d_tiles) cudaFree(c->d_tiles);
+      c->d_tiles = nullptr;
+      c->tiles_cap = 0;
+      e = cudaMalloc(&c->d_tiles, sizeof(int2) * tiles.size());
+      if (e != cudaSuccess) return cuda_fail(c, e, "range tiles");
+      c->tiles_cap = tiles.size();
+    }
+    if (!tiles.empty()) {
+      cudaError_t e = cudaMemcpyAsync(c->d_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice,
+                                      stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "range tiles");
+    }
+    k.tiles = c->d_tiles;
+    k.n_tiles = static_cast<int32_t>(tiles.size());
+  }
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   k.gates_per_block = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads;
   // the (tile, net) first-event table, when it stays within kTileFirstMaxEntries
@@ -273,7 +314,8 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     if (c->d_tile_first) k.tile_first = c->d_tile_first;
   }
   // the glitch widths of the window's events, within kGlitchPwMaxEvents
-  if (n_event > 0 && n_event <= kGlitchPwMaxEvents) {
+  // (cycle ranges classify the few events they walk online instead)
+  if (!ranges && n_event > 0 && n_event <= kGlitchPwMaxEvents) {
     if (n_event > c->glitch_pw_cap) {
       cudaError_t e = cudaStreamSynchronize(stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -287,15 +329,16 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     }
     if (c->d_glitch_pw) k.glitch_pw = c->d_glitch_pw;
   }
-  if (c->cfg.sort_by_work && c->d_order_work) k.order = c->d_order_work;
-  if (runs) k.pclk = c->d_pclk;
+  const bool sorted = c->cfg.sort_by_work && c->d_order_work && !ranges;
+  if (sorted) k.order = c->d_order_work;
+  if (runs && !standalone) k.pclk = c->d_pclk;
   if (enqueue_prep) {
     cudaError_t e = cudaSuccess;
     if (k.tile_first) e = launch_tile_first(k, nullptr, c->d_tile_first, stream);
     if (e == cudaSuccess && k.glitch_pw) e = launch_glitch_pw(k, nullptr, c->d_glitch_pw, stream);
     if (e == cudaSuccess && k.pclk) e = launch_pclk(k, nullptr, c->d_clk_nets, c->n_clk_nets, c->d_pclk, stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tile index");
-    if (c->cfg.sort_by_work && c->d_order_work) {
+    if (sorted) {
       e = sort_cells_by_work(k, c->d_order, P.bucket_begin[3], P.bucket_begin, c->d_keys_in, c->d_keys_out,
                              c->d_order_work, c->d_sort_temp, c->sort_temp_bytes, stream);
       if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
@@ -333,16 +376,20 @@ void commit_window(gtp_ctx* c, int64_t t_hi) {
 
 gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
                       const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
-                      int64_t t_lo, int64_t t_hi) {
+                      int64_t t_lo, int64_t t_hi, const std::vector<int64_t>* ranges = nullptr) {
   KParams k;
-  gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, c->stream, &k);
+  gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, c->stream, &k, true, ranges);
   if (st != GTP_OK) return st;
+  if (k.n_tiles <= 0) {  // cycle ranges outside the window: nothing to walk
+    commit_window(c, t_hi);
+    return GTP_OK;
+  }
   const Packed& P = c->P;
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   const bool counts = c->cfg.collect_counts != 0;
   // density split: cells whose measured events per tile exceed split_events
   // are walked by several threads, each over part of the tile's cycles
-  if (c->d_item_off && c->cfg.sort_by_work && c->d_order_work && P.bucket_begin[3] > 0) {
+  if (!ranges && c->d_item_off && c->cfg.sort_by_work && c->d_order_work && P.bucket_begin[3] > 0) {
     const int32_t se = c->cfg.split_events > 0 ? c->cfg.split_events : kDefaultSplitEvents;
     const int64_t last_tick = std::min<int64_t>(k.t_hi - 1, k.tmax);
     const int64_t n_cyc = std::max<int64_t>(1, last_tick / k.tpc + 1 - k.cyc0);
@@ -628,6 +675,28 @@ gtp_status gtp_push_events_device(gtp_ctx* c, const gtp_events* ev) {
   }
   return run_window(c, ev->net_off, ev->time, ev->value_packed, ev->net_base, ev->n_event,
                     ev->t_lo, ev->t_hi);
+}
+
+gtp_status gtp_push_events_device_ranges(gtp_ctx* c, const gtp_events* ev, const int64_t* cycle_ranges,
+                                         int32_t n_ranges) {
+  if (!c || !ev) return GTP_EINVAL;
+  if (ev->n_event < 0 || !ev->net_off || (ev->n_event > 0 && (!ev->time || !ev->value_packed)) || n_ranges < 0 ||
+      (n_ranges > 0 && !cycle_ranges)) {
+    c->err = "events or ranges: missing arrays";
+    return GTP_EINVAL;
+  }
+  std::vector<int64_t> r(cycle_ranges, cycle_ranges + 2 * static_cast<size_t>(n_ranges));
+  for (int32_t i = 0; i < n_ranges; ++i) {
+    if (r[2 * i] < 0 || r[2 * i + 1] <= r[2 * i] || (i > 0 && r[2 * i] < r[2 * i - 1])) {
+      c->err = "cycle ranges must be non-empty, ascending and disjoint";
+      return GTP_EINVAL;
+    }
+  }
+  if (n_ranges > 0 && (r[0] * c->P.tpc < ev->t_lo || (ev->t_hi < INT64_MAX / 2 && r.back() * c->P.tpc > ev->t_hi))) {
+    c->err = "cycle ranges must lie within the window [t_lo, t_hi)";
+    return GTP_EINVAL;
+  }
+  return run_window(c, ev->net_off, ev->time, ev->value_packed, ev->net_base, ev->n_event, ev->t_lo, ev->t_hi, &r);
 }
 
 gtp_status gtp_sync(gtp_ctx* c) {

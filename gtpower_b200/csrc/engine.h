@@ -187,6 +187,14 @@ struct KParams {
   const int32_t* cell_cgroup;       // [n_cell] group of each cell, or null
   int32_t n_cgroup;
   unsigned long long* cyc_acc_g;    // [n_cgroup][6][n_period+1]
+  // cycle ranges (optional): tile t covers cycles [tiles[t].x, tiles[t].x +
+  // tiles[t].y); null = tile t covers cycles cyc0 + t * cycles_per_tile ...
+  const int2* tiles;
+  // the window is evaluated on its own (after a gap, or over cycle ranges):
+  // each tile's leakage starts at its first tick and ends at its last
+  // instead of carrying over from the windows before
+  int32_t standalone;
+  int32_t standalone_pad;
   // density split (optional, one-window walk only): item_off[k] = first walk
   // item of the cell at walk-order position k (exclusive prefix over
   // positions of the number of threads that walk it per tile), n_cell + 1

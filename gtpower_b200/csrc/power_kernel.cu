@@ -336,7 +336,11 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   bins.sc = reinterpret_cast<uint32_t*>(smem + nset * nslot * ct);
   bins.off = 0;
   bins.g = 0;
-  bins.c_lo = p.cyc0 + static_cast<int64_t>(tile) * ct;
+  // the tile's cycles [c_lo, c_lo + ct_tile): from the range table, or the
+  // window's regular tiling
+  const int2 tdesc = p.tiles ? p.tiles[tile] : make_int2(0, 0);
+  bins.c_lo = p.tiles ? static_cast<int64_t>(tdesc.x) : p.cyc0 + static_cast<int64_t>(tile) * ct;
+  const int64_t ct_tile = p.tiles ? static_cast<int64_t>(tdesc.y) : ct;
   bins.ct = ct;
   for (int64_t k = threadIdx.x; k < nset * nslot * ct; k += blockDim.x) smem[k] = 0ull;
   if (COUNTS)
@@ -369,10 +373,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   // T0's offset within cycle c_lo: event cycles follow from 32-bit offsets
   const uint32_t off0 = static_cast<uint32_t>(T0 - bins.c_lo * p.tpc);
   const uint32_t tpc32 = static_cast<uint32_t>(p.tpc);
-  const bool last_tile = (tile == p.n_tiles - 1);
-  const int64_t T1 = last_tile ? min(p.t_hi, p.tmax + 1) : min(p.t_hi, (bins.c_lo + ct) * p.tpc);
+  // the tile ends at its last cycle's end, or past time_max (events at
+  // time_max belong to the trace) when it reaches the trace's end
+  const int64_t t_end = (bins.c_lo + ct_tile) * p.tpc;
+  const int64_t T1 = t_end > p.tmax ? min(p.t_hi, p.tmax + 1) : min(p.t_hi, t_end);
   const uint32_t span = static_cast<uint32_t>(T1 > T0 ? T1 - T0 : 0);
-  const bool owns_initial = (tile == 0) && (p.t_lo == 0);
+  const bool standalone = p.standalone != 0;
+  const bool owns_initial = !standalone && bins.c_lo == 0 && (p.t_lo == 0);
   const double P = p.period_d;
   // clock runs: a periodic pin's edges exist from tick max(t_lo, 1) on
   // (r_exist relative to T0); the tile holds those before span
@@ -725,6 +732,13 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       acc_add(4, static_cast<double>(leak_cur) * static_cast<double>(p.tmax));
       add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak_cur) * P, p.fx_leak));
     }
+    // per-cell leakage of a level change at tick t: its level times the
+    // ticks to the end of what the walk accounts (time_max, or for a
+    // standalone window the end of this part of the tile)
+    const int64_t leak_end = standalone ? min(T0 + static_cast<int64_t>(s1r), p.tmax) : p.tmax;
+    // standalone: the fixed-point level this part has added, removed
+    // exactly (integer for integer) at its end
+    unsigned long long lvl_fx = 0ull;
     // drift path: a segment whose seconds cycle precedes its tick cycle
     // needs its end before its correction is known
     bool pend = false;
@@ -743,6 +757,49 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       }
       pend = false;
     };
+    // the cell's leakage changes from leak_cur to leak_new at tick cur_abs
+    // (tick cycle cyc, tile cycle cq): its share of the cycle the tick lies in
+    // (in seconds), the level from the next cycle on, and with DRIFT the
+    // correction where the tick and seconds cycles differ
+    auto level_change = [&](int64_t cur_abs, int64_t cyc, uint32_t cq, float leak_new) {
+      const int64_t s = DRIFT ? seconds_cycle(p, cur_abs, cyc) : cyc;
+      if (leak_new != leak_cur) {
+        const double dl = static_cast<double>(leak_new) - static_cast<double>(leak_cur);
+        const double cur_s = static_cast<double>(cur_abs) * p.ts;
+        const double end_s = fmin(static_cast<double>(s + 1) * P, p.tmax_s);
+        const unsigned long long lv = to_fx(dl * P, p.fx_leak);
+        if (DRIFT) {
+          add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
+          add_bin(p, bins, kLeakLevel, s + 1, lv);
+        } else {  // s is the tick cycle c_lo + cq
+          add_bin_k(p, bins, kLeakPart, cq, to_fx(dl * (end_s - cur_s), p.fx_leak));
+          add_bin_k(p, bins, kLeakLevel, cq + 1, lv);
+        }
+        lvl_fx += lv;
+        acc_add(4, dl * static_cast<double>(leak_end - cur_abs));
+      }
+      if (DRIFT && s != cyc) {
+        if (s == cyc + 1) {
+          const double w = static_cast<double>(cur_abs) * p.ts - static_cast<double>(cyc + 1) * P;
+          const double v = static_cast<double>(leak_new);
+          add_bin(p, bins, kLeakPart, cyc, to_fx(-v * w, p.fx_leak));
+          add_bin(p, bins, kLeakPart, cyc + 1, to_fx(v * w, p.fx_leak));
+        } else {
+          pend = true;
+          pend_p = cur_abs;
+          pend_c0 = cyc;
+          pend_v = leak_new;
+        }
+      }
+      leak_cur = leak_new;
+    };
+    if (standalone) {
+      // the leakage of a standalone part starts at its first tick
+      const uint32_t k0 = udiv32(s0r + off0, tpc32, p.tpc_magic);
+      const float l0 = leak_cur;
+      leak_cur = 0.0f;
+      level_change(T0 + static_cast<int64_t>(s0r), bins.c_lo + k0, k0, l0);
+    }
 
     while (true) {
       uint32_t cur = kRelInf;
@@ -831,35 +888,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
 
       // leakage: level change at cur
       if (DRIFT && pend) apply_pending(cur_abs);
-      const float leak_new = leak_of(ones);
-      const int64_t s = DRIFT ? seconds_cycle(p, cur_abs, cyc) : cyc;
-      if (leak_new != leak_cur) {
-        const double dl = static_cast<double>(leak_new) - static_cast<double>(leak_cur);
-        const double cur_s = static_cast<double>(cur_abs) * p.ts;
-        const double end_s = fmin(static_cast<double>(s + 1) * P, p.tmax_s);
-        if (DRIFT) {
-          add_bin(p, bins, kLeakPart, s, to_fx(dl * (end_s - cur_s), p.fx_leak));
-          add_bin(p, bins, kLeakLevel, s + 1, to_fx(dl * P, p.fx_leak));
-        } else {  // s is the tick cycle c_lo + cq
-          add_bin_k(p, bins, kLeakPart, cq, to_fx(dl * (end_s - cur_s), p.fx_leak));
-          add_bin_k(p, bins, kLeakLevel, cq + 1, to_fx(dl * P, p.fx_leak));
-        }
-        acc_add(4, dl * static_cast<double>(p.tmax - cur_abs));
-      }
-      if (DRIFT && s != cyc) {
-        if (s == cyc + 1) {
-          const double w = static_cast<double>(cur_abs) * p.ts - static_cast<double>(cyc + 1) * P;
-          const double v = static_cast<double>(leak_new);
-          add_bin(p, bins, kLeakPart, cyc, to_fx(-v * w, p.fx_leak));
-          add_bin(p, bins, kLeakPart, cyc + 1, to_fx(v * w, p.fx_leak));
-        } else {
-          pend = true;
-          pend_p = cur_abs;
-          pend_c0 = cyc;
-          pend_v = leak_new;
-        }
-      }
-      leak_cur = leak_new;
+      level_change(cur_abs, cyc, cq, leak_of(ones));
 
       // energies of the triggered pins, in pin order, from the pre-step state
       uint32_t tb = trig;
@@ -996,6 +1025,27 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
     }
 
     if (pkbit) pclk_close(pclk_jend(), ones & ~pkbit);
+    // ... and ends at its last tick, unless that lies past time_max: the
+    // level it added is taken back integer for integer, from the cycle the
+    // tick starts (without drift, on a cycle boundary) or from the next one,
+    // after the rest of the tick's cycle at the final level
+    if (standalone && T0 + static_cast<int64_t>(s1r) <= p.tmax) {
+      const int64_t t1 = T0 + static_cast<int64_t>(s1r);
+      if (DRIFT && pend) apply_pending(t1);
+      const uint32_t k = udiv32(s1r + off0, tpc32, p.tpc_magic);
+      const uint32_t h = s1r + off0 - k * tpc32;
+      const int64_t cyc1 = bins.c_lo + k;
+      const int64_t s1 = DRIFT ? seconds_cycle(p, t1, cyc1) : cyc1;
+      if (!DRIFT && h == 0) {
+        add_bin_k(p, bins, kLeakLevel, k, 0ull - lvl_fx);
+      } else {
+        const double cur_s = static_cast<double>(t1) * p.ts;
+        const double end_s = fmin(static_cast<double>(s1 + 1) * P, p.tmax_s);
+        add_bin(p, bins, kLeakPart, s1, to_fx(-static_cast<double>(leak_cur) * (end_s - cur_s), p.fx_leak));
+        add_bin(p, bins, kLeakLevel, s1 + 1, 0ull - lvl_fx);
+      }
+      leak_cur = 0.0f;
+    }
 
     if (DRIFT && pend) {
       // end of the pending segment: the cell's next event, or time_max
@@ -1109,7 +1159,8 @@ __global__ void tile_first_kernel(const KParams pv, const KParams* __restrict__ 
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t tile = i / nn;
     const int32_t net = static_cast<int32_t>(i - tile * nn);
-    const int64_t T0 = max(p.t_lo, (p.cyc0 + tile * p.cycles_per_tile) * p.tpc);
+    const int64_t c_lo = p.tiles ? static_cast<int64_t>(p.tiles[tile].x) : p.cyc0 + tile * p.cycles_per_tile;
+    const int64_t T0 = max(p.t_lo, c_lo * p.tpc);
     const int64_t a = p.net_off[net], e = p.net_off[net + 1];
     int64_t l = a, r = e;
     if (a < 0 || e < a || e > p.n_event) {  // reported by the walk

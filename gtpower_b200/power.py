@@ -155,6 +155,24 @@ class B200Power:
         _abi.check(_abi.lib().gtp_push_events_device(self.ctx, C.byref(e)), self.ctx)
         self._results = None
 
+    def push_device_ranges(self, n_event: int, d_net_off: int, d_time: int, d_packed: int, ranges,
+                           d_net_base: int = 0, t_lo: int = 0, t_hi: int = np.iinfo(np.int64).max) -> None:
+        """Evaluates only the cycle ranges [(c0, c1), ...] (ascending,
+        disjoint) of a device-resident window, in one pass; per-cycle power
+        of other cycles stays zero."""
+        r = np.ascontiguousarray(np.asarray(ranges, dtype=np.int64).reshape(-1))
+        e = _abi.gtp_events()
+        e.n_event = n_event
+        e.net_off = d_net_off
+        e.time = d_time
+        e.value_packed = d_packed
+        e.net_base = d_net_base or None
+        e.t_lo = t_lo
+        e.t_hi = t_hi
+        _abi.check(_abi.lib().gtp_push_events_device_ranges(self.ctx, C.byref(e), r.ctypes.data_as(C.c_void_p),
+                                                            int(r.shape[0] // 2)), self.ctx)
+        self._results = None
+
     @property
     def stream(self) -> int:
         """cudaStream_t of the context, as an integer handle."""

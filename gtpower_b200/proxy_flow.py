@@ -133,19 +133,18 @@ def engine_time(design, windows: list[DeviceWindow], c_lo: int, c_hi: int, **eng
 
 def engine_spot(design, windows: list[DeviceWindow], ranges: list[tuple[int, int]], **eng_kw):
     """The plain path over disjoint ascending cycle ranges only (audit and
-    fallback): per-cycle totals (zero outside) and device seconds."""
+    fallback): per-cycle totals (zero outside) and device seconds. Each
+    window holding some of the ranges is walked once, over those ranges only
+    (gtp_push_events_device_ranges)."""
     torch = _torch()
-    tpc = None
     with B200Power(design, **eng_kw) as eng:
-        tpc = eng.ticks_per_cycle
         s = torch.cuda.ExternalStream(eng.stream)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(s)
-        for c0, c1 in ranges:
-            for w in windows:
-                lo, hi = max(c0, w.c_lo), min(c1, w.c_hi)
-                if lo < hi:
-                    w.push(eng, lo * tpc, hi * tpc)
+        for w in windows:
+            mine = [(max(c0, w.c_lo), min(c1, w.c_hi)) for c0, c1 in ranges if max(c0, w.c_lo) < min(c1, w.c_hi)]
+            if mine:
+                w.push_ranges(eng, mine)
         b.record(s)
         eng.sync()
         res = eng.fetch()

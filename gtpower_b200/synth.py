@@ -453,6 +453,12 @@ class DeviceWindow:
                         self.net_base.data_ptr(), self.t_lo if t_lo is None else t_lo,
                         self.t_hi if t_hi is None else t_hi)
 
+    def push_ranges(self, eng, ranges) -> None:
+        """Evaluates only the cycle ranges [(c0, c1), ...] of this window
+        (ascending, disjoint, inside it) in one pass."""
+        eng.push_device_ranges(self.n_event, self.net_off.data_ptr(), self.time.data_ptr(), self.packed.data_ptr(),
+                               ranges, self.net_base.data_ptr(), self.t_lo, self.t_hi)
+
 
 class DeviceStream:
     """Windows of a `Trace` generated on the GPU, identical to `Stream`'s."""

@@ -261,12 +261,29 @@ gtp_status  gtp_reset(gtp_ctx* ctx);
  * device and evaluates it. Windows must come in time order without overlap.
  * Gaps are allowed: cycles no window covers keep zero per-cycle power, and
  * per-cell values then cover the evaluated windows only (a spot check of
- * selected cycle ranges, e.g. the learned proxy's audit sample). */
+ * selected cycle ranges, e.g. the learned proxy's audit sample). A window
+ * after a gap (or a first window with t_lo > 0) is evaluated on its own: its
+ * leakage starts at t_lo from the state its context gives and ends at t_hi. */
 gtp_status  gtp_push_events(gtp_ctx* ctx, const gtp_events* ev);
 
 /* Same, with events already in device memory (time, value_packed, net_off,
  * net_base are device pointers). Nothing is copied. */
 gtp_status  gtp_push_events_device(gtp_ctx* ctx, const gtp_events* d_ev);
+
+/* Evaluates only cycles [cycle_ranges[2k], cycle_ranges[2k+1]) of a device
+ * window (ranges ascending, disjoint, within [t_lo, t_hi)), in one pass:
+ * spot checks of selected cycles, such as the learned proxy's audit sample
+ * and its out-of-range cycles, without walking the rest of the window. The
+ * window lists its events as for gtp_push_events_device; the state at each
+ * range's start comes from the events before it. Per-cycle power of other
+ * cycles stays zero (leakage included: each range is evaluated on its own),
+ * per-cell values and counts cover the ranges only, and clock pins are walked
+ * edge by edge. The window counts as pushed: later windows follow t_hi.
+ * Where the design's tick and seconds cycle boundaries drift apart, the
+ * leakage of a cycle that straddles a range's edge in seconds covers only
+ * the range's part of it (as for a window pushed after a gap). */
+gtp_status  gtp_push_events_device_ranges(gtp_ctx* ctx, const gtp_events* d_ev, const int64_t* cycle_ranges,
+                                          int32_t n_ranges);
 
 /* Waits for all queued work. */
 gtp_status  gtp_sync(gtp_ctx* ctx);
