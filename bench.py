@@ -70,7 +70,7 @@ def parse():
                          "several threads (0: the engine's default, -1: off)")
     ap.add_argument("--no-clock-runs", action="store_true",
                     help="walk periodic clock pins edge by edge instead of as runs of whole cycles")
-    ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream"],
+    ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream", "gemm"],
                     help="flat: the plain walk (default); proxy: the learned per-cycle power proxy "
                          "against the plain walk on a phased-unit trace; batch: 64 uneven traces x "
                          "3 corners in persistent batched launches")
@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--proxy-window", type=int, default=2_000)
     ap.add_argument("--proxy-epochs", type=int, default=40)
     ap.add_argument("--proxy-inputs", type=int, default=4096)
+    ap.add_argument("--gemm-rows", type=int, default=80_000,
+                    help="gemm: rows (cycles) of the proxy's inference, and of each single GEMM timed")
     return ap.parse_args()
 
 
@@ -236,6 +238,71 @@ def run_proxy(args):
                     "select": rep.select_s},
         "training": {"epochs": rep.epochs, "loss_first": rep.losses[0], "loss_last": rep.losses[-1],
                      "ridge_lambda": rep.ridge_lambda},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"{kind} (MEASURED_PEAKS.json bf16_tflops)" if kind == "measured" else "fallback",
+                     "kernel": "gemm_kernel (3 layers, inference)"},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gemm(args):
+    """The proxy's inference on the tcgen05 GEMM, on its own: the MLP
+    4096-512-512-33 over --gemm-rows cycles of random toggle bits (the
+    gtp_proxy_predict path: three GEMMs with fused bias/ReLU and BF16
+    activations), and each layer's shape as one GEMM with an FP32 output
+    (gtp_bf16_gemm). Device time by CUDA events on the launching streams,
+    after warm-up."""
+    import torch
+    from gtpower_b200 import proxy as px
+    torch.cuda.set_device(0)
+    m, k_in, h, n_out = args.gemm_rows, args.proxy_inputs, 512, 33
+    g = torch.Generator(device="cuda").manual_seed(20261203 + 5)
+    x = (torch.rand(m, k_in, device="cuda", generator=g) < 0.2).to(torch.bfloat16)
+    net = px.PowerProxy(n_in=k_in, n_hidden=h, n_out=n_out)
+    s = net.stream
+    out = torch.empty((m, n_out), dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(0)
+    sampler.start()
+    for _ in range(args.warmup):
+        net.predict(x, out=out)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in evs:
+        a.record(s)
+        net.predict(x, out=out, sync=False)
+        b.record(s)
+    s.synchronize()
+    pred_ms = [a.elapsed_time(b) for a, b in evs]
+    op = (n_out + 7) // 8 * 8
+    flops = 2.0 * m * (k_in * h + h * h + h * op)
+    layers = {}
+    for name, (kk, nn) in {"layer1": (k_in, h), "layer2": (h, h), "layer3": (h, op)}.items():
+        a_ = torch.randn(m, kk, device="cuda", generator=g).to(torch.bfloat16)
+        b_ = torch.randn(nn, kk, device="cuda", generator=g).to(torch.bfloat16)
+        for _ in range(args.warmup):
+            px.bf16_gemm(a_, b_)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            px.bf16_gemm(a_, b_)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        layers[name] = {"m": m, "n": nn, "k": kk, "ms": ms, "tflops": 2.0 * m * nn * kk / ms / 1e9}
+        del a_, b_
+    clocks = sampler.stop()
+    net.close()
+    peak, kind = measured_peak_tensor()
+    ms = float(np.median(pred_ms))
+    achieved = flops / ms / 1e9
+    line = {
+        "metric": f"proxy inference TFLOP/s (MLP {k_in}-512-512-33 over {m} cycles, tcgen05 BF16 GEMMs)",
+        "value": achieved, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic", "config": {"workload": f"random toggle bits {m} x {k_in} (p=0.2), random weights"},
+        "cycles_per_s": m / (ms / 1e3), "single_gemm_fp32_out": layers,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": f"{kind} (MEASURED_PEAKS.json bf16_tflops)" if kind == "measured" else "fallback",
@@ -652,6 +719,10 @@ def main():
     if args.workload == "stream":
         if rank == 0:
             run_stream(args)
+        return
+    if args.workload == "gemm":
+        if rank == 0:
+            run_gemm(args)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -122,7 +122,8 @@ EXPORTED = sorted([
     "gtp_evaluate_noalloc", "gtp_pack_values",
     "gtp_set_cycle_groups", "gtp_n_cycle_groups", "gtp_fetch_cycle_groups", "gtp_clock_run_nets",
     "gtp_walk_items", "gtp_set_cell_range", "gtp_accumulator_bytes", "gtp_export_accumulators",
-    "gtp_import_accumulators", "gtp_push_events_device_ranges", "gtp_write_cell_power", "gtp_write_per_cycle_waveform",
+    "gtp_import_accumulators", "gtp_push_events_device_ranges", "gtp_write_cell_power",
+    "gtp_vcd_create", "gtp_vcd_parse", "gtp_vcd_fetch", "gtp_vcd_stats", "gtp_vcd_last_error", "gtp_vcd_destroy", "gtp_write_per_cycle_waveform",
     "gtp_batch_config_default", "gtp_batch_create", "gtp_batch_destroy", "gtp_batch_last_error",
     "gtp_batch_push_device", "gtp_batch_sync", "gtp_batch_get_stream", "gtp_batch_stats",
     "gtp_proxy_config_default", "gtp_proxy_create", "gtp_proxy_destroy", "gtp_proxy_last_error",
@@ -201,6 +202,18 @@ def lib() -> C.CDLL:
     L.gtp_import_accumulators.restype = C.c_int32
     L.gtp_push_events_device_ranges.argtypes = [C.c_void_p, C.POINTER(gtp_events), _P, C.c_int32]
     L.gtp_push_events_device_ranges.restype = C.c_int32
+    L.gtp_vcd_create.argtypes = [C.c_char_p, _P, C.c_int32, _P, _P, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.gtp_vcd_create.restype = C.c_int32
+    L.gtp_vcd_parse.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.POINTER(gtp_events), C.POINTER(C.c_int64)]
+    L.gtp_vcd_parse.restype = C.c_int32
+    L.gtp_vcd_fetch.argtypes = [C.c_void_p, _P, _P, _P]
+    L.gtp_vcd_fetch.restype = C.c_int32
+    L.gtp_vcd_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.gtp_vcd_stats.restype = C.c_int32
+    L.gtp_vcd_last_error.argtypes = [C.c_void_p]
+    L.gtp_vcd_last_error.restype = C.c_char_p
+    L.gtp_vcd_destroy.argtypes = [C.c_void_p]
+    L.gtp_vcd_destroy.restype = None
     L.gtp_write_cell_power.argtypes = [C.c_char_p, C.c_int32, _P, _P, _P, _P, C.c_char_p]
     L.gtp_write_cell_power.restype = C.c_int32
     L.gtp_write_per_cycle_waveform.argtypes = [C.c_char_p, C.c_int64, _P, C.c_char_p, C.c_char_p]

@@ -17,7 +17,7 @@ LIB = os.path.join(LIBDIR, "libgtpb200.so")
 SYNTH_LIB = os.path.join(LIBDIR, "libgtpb200_synth.so")
 SYNTHDEV_LIB = os.path.join(LIBDIR, "libgtpb200_synthdev.so")
 
-ENGINE_SOURCES = ["abi.cu", "power_kernel.cu", "pack.cpp", "writers.cpp", "umma_gemm.cu", "proxy.cu"]
+ENGINE_SOURCES = ["abi.cu", "power_kernel.cu", "pack.cpp", "writers.cpp", "vcd_gpu.cu", "umma_gemm.cu", "proxy.cu"]
 SYNTH_SOURCES = ["synth.cpp"]
 SYNTHDEV_SOURCES = ["synth_dev.cu"]
 

@@ -4,7 +4,8 @@ Follows power/VcdReader.cc and power/Vcd.cc:
   - values are upper-cased; scalar 0/1/X/U/Z changes are stored
     (VcdReader::parseVarValues, VcdReader.cc:247-301);
   - a vector value `b...` whose first digit is x/u/z becomes bus value 0;
-    otherwise the leading binary digits are read (strtol base 2);
+    otherwise the leading binary digits are read (strtol base 2, which
+    saturates at 2^63 - 1);
   - real values are skipped;
   - a change equal to the previous value of the same id is dropped, and an
     initial value is inserted at tick 0 when the first change is later
@@ -52,9 +53,26 @@ def _open(path):
 
 
 def read(path: str) -> Vcd:
-    v = Vcd()
     with _open(path) as f:
-        toks = f.read().split()
+        return read_text(f.read())
+
+
+def split_header(raw: bytes) -> tuple[bytes, bytes]:
+    """(header, body) of a VCD file's bytes: the body starts after the
+    `$end` that closes `$enddefinitions`."""
+    m = re.search(rb"(?:^|\s)\$enddefinitions(?=\s|$)", raw)
+    if not m:
+        return raw, b""
+    e = re.search(rb"(?:^|\s)\$end(?=\s|$)", raw[m.end():])
+    if not e:
+        return raw, b""
+    cut = m.end() + e.end()
+    return raw[:cut], raw[cut:]
+
+
+def read_text(text: str) -> Vcd:
+    v = Vcd()
+    toks = text.split()
     n = len(toks)
     i = 0
     scope: list[str] = []
@@ -121,8 +139,10 @@ def read(path: str) -> Vcd:
             if c1 in "XUZ":
                 bus = 0
             else:
+                # the leading binary digits, as strtol reads them (saturated
+                # at its largest value)
                 m = re.match(r"[01]*", t[1:])
-                bus = int(m.group(0), 2) if m.group(0) else 0
+                bus = min(int(m.group(0), 2), (1 << 63) - 1) if m.group(0) else 0
             ts, cs, bs, w = v.values[vid]
             if not bs or bs[-1] != bus or not ts:
                 if not ts and time != 0:

@@ -447,6 +447,44 @@ gtp_status  gtp_write_cell_power(const char* path, int32_t n_cell, const float* 
 gtp_status  gtp_write_per_cycle_waveform(const char* path, int64_t n_period, const float* cycle5,
                                          const char* top_name, const char* sep);
 
+/* VCD value-change ingest on the GPU. Replaces the reference's host parse
+ * of the VCD body (VcdReader::parseVarValues, power/VcdReader.cc:247-301),
+ * its per-var value store (Vcd::varAppendValue / varAppendBusValue,
+ * power/Vcd.cc:204-234; bus bits as VcdValue::value, :271-277) and the
+ * per-pin event-buffer build (CudaPower::getGateWaveformRangeMultiThread,
+ * power/cuda/CudaPower.cu:1874-2086). The caller parses the header ($var
+ * declarations are few) and passes:
+ *   the distinct id codes: id_chars[id_off[i] .. id_off[i+1]) for i < n_id;
+ *   the sources: net s of the output CSR lists bit src_bit[s] of id
+ *     src_id[s] (bit 0 for scalars; for a vector, bit b of its value with
+ *     b = 0 the LSB).
+ * gtp_vcd_parse then reads a body (host bytes, the text after
+ * $enddefinitions ... $end) with the reference's rules: upper-cased first
+ * characters; scalar changes 0/1/x/u/z<id> (u read as X); vector changes
+ * b<digits> <id>, a value whose first digit is x/u/z being 0, else the
+ * leading binary digits as strtol reads them; r<real> <id> skipped; a
+ * change equal to the id's previous one dropped; an X (scalars) or 0
+ * (vectors) inserted at tick 0 before an id's first change when that comes
+ * later; time_max = the last time stamp. It fills *d_out with device
+ * arrays (t_lo 0, t_hi INT64_MAX, no net_base) that stay valid until the
+ * next parse or gtp_vcd_destroy, ready for gtp_push_events_device.
+ * GTP_EINVAL on an undeclared id, a time stamp that is not a decimal number
+ * or an id that takes both scalar and vector changes (message in
+ * gtp_vcd_last_error). Work runs on the reader's own stream; the call
+ * returns when the CSR is complete. */
+typedef struct gtp_vcd gtp_vcd;
+gtp_status  gtp_vcd_create(const char* id_chars, const int32_t* id_off, int32_t n_id, const int32_t* src_id,
+                           const int32_t* src_bit, int32_t n_src, int32_t cuda_device_id, gtp_vcd** out);
+gtp_status  gtp_vcd_parse(gtp_vcd* vcd, const char* body, int64_t n_bytes, gtp_events* d_out,
+                          int64_t* time_max);
+/* Host copies of the last parse's CSR (net_off [n_src+1], time [n_event],
+ * packed [ceil(n_event/16)]; any may be NULL). */
+gtp_status  gtp_vcd_fetch(gtp_vcd* vcd, int64_t* net_off, int64_t* time, uint32_t* packed);
+/* Tokens and value changes (before repeat dropping) of the last parse. */
+gtp_status  gtp_vcd_stats(const gtp_vcd* vcd, int64_t* n_token, int64_t* n_change);
+const char* gtp_vcd_last_error(const gtp_vcd* vcd);
+void        gtp_vcd_destroy(gtp_vcd* vcd);
+
 /* Packs one value per byte (0..3) into the 2-bit layout of value_packed. */
 void        gtp_pack_values(const uint8_t* values, int64_t n, uint32_t* packed);
 
