@@ -538,12 +538,12 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     }
     if (e != cudaSuccess) goto cuda_err;
   }
-  // fixed-point scales: a per-cycle dynamic bin holds at most 2^30 events of
-  // max|E| (resolution max|E| * 2^-32), leakage bins max|leak| * period * 4 *
-  // (n_cell + 1)
-  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 30));
-  c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * 4.0 *
-                                 (static_cast<double>(P.n_cell) + 1.0));
+  // fixed-point scales: one event's energy, and one level change's leakage
+  // over a period, are at most 2^24 units (resolution max|E| * 2^-24 and
+  // max|leak| * period * 2^-24), so that most adds to a shared bin stay
+  // within its low 32-bit word; a 64-bit bin then holds 2^38 of them
+  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 38));
+  c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * std::ldexp(1.0, 38));
   if (gtp_reset(c) != GTP_OK) { set_err(c->err); free_all(c); delete c; return GTP_ECUDA; }
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) goto cuda_err;

@@ -133,6 +133,20 @@ __device__ __forceinline__ T sel(const T (&a)[N], int i) {
   return r;
 }
 
+// 64-bit fixed-point add to a shared-memory bin as two 32-bit atomics: the
+// low word's add returns the old value, so its carry is known exactly and
+// goes to the high word (with the value's own high word) only when that sum
+// is non-zero. The bin, read as one 64-bit word, holds the exact sum modulo
+// 2^64 in any order of adds. On sm_100 a 32-bit shared atomic costs a small
+// fraction of a 64-bit one, and most adds need one.
+__device__ __forceinline__ void shared_add64(unsigned long long* a, unsigned long long x) {
+  uint32_t* w = reinterpret_cast<uint32_t*>(a);
+  const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
+  const uint32_t old = atomicAdd(w, xl);
+  const uint32_t h = xh + (old + xl < old ? 1u : 0u);
+  if (h) atomicAdd(w + 1, h);
+}
+
 struct Bins {
   unsigned long long* s;   // [sets][slots][ct] fixed-point energies
   uint32_t* sc;            // [2][ct] counts
@@ -155,7 +169,7 @@ __device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, 
   if (x == 0ull) return;
   const int64_t k = c - b.c_lo;
   if (k >= 0 && k < b.ct && b.off >= 0) {
-    atomicAdd(b.s + b.off + q * b.ct + k, x);
+    shared_add64(b.s + b.off + q * b.ct + k, x);
   } else {
     const int64_t cc = c < 0 ? p.n_period : (c < p.n_period ? c : p.n_period);
     atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
@@ -169,7 +183,7 @@ __device__ __forceinline__ void add_bin_k(const KParams& p, const Bins& b, int q
                                           unsigned long long x) {
   if (x == 0ull) return;
   if (k < static_cast<uint32_t>(b.ct) && b.off >= 0)
-    atomicAdd(b.s + b.off + static_cast<uint32_t>(q) * static_cast<uint32_t>(b.ct) + k, x);
+    shared_add64(b.s + b.off + static_cast<uint32_t>(q) * static_cast<uint32_t>(b.ct) + k, x);
   else
     add_bin(p, b, q, b.c_lo + k, x);
 }
@@ -707,12 +721,12 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
         acc_add(4, n * dl * static_cast<double>(pB - pA));
         unsigned long long* run = bins.s + bins.off;
         if (e2) {
-          atomicAdd(run + kIntRun * ct + k1, e2);
-          if (k2 < ct) atomicAdd(run + kIntRun * ct + k2, 0ull - e2);
+          shared_add64(run + kIntRun * ct + k1, e2);
+          if (k2 < ct) shared_add64(run + kIntRun * ct + k2, 0ull - e2);
         }
         if (l2) {
-          atomicAdd(run + kLeakRun * ct + k1, l2);
-          if (k2 < ct) atomicAdd(run + kLeakRun * ct + k2, 0ull - l2);
+          shared_add64(run + kLeakRun * ct + k1, l2);
+          if (k2 < ct) shared_add64(run + kLeakRun * ct + k2, 0ull - l2);
         }
         if (COUNTS) {
           n_ev += 2 * (k2 - k1);
