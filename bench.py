@@ -802,8 +802,9 @@ def main():
         return ev0, ev1
 
     # per step: tile_first, glitch_pw, pclk, work_keys (then the library's
-    # radix sort), the walk (one pin bucket here), finalize_cells, finalize_cycles
-    launches_per_step = 7
+    # radix sort), split_count (then the library's scan), the walk (one pin
+    # bucket here), finalize_cells, finalize_cycles
+    launches_per_step = 8
     from gtpower_b200 import _abi
     import ctypes as C
 
