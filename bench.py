@@ -68,6 +68,10 @@ def parse():
     ap.add_argument("--split-events", type=int, default=0,
                     help="density split: events per thread and tile above which a cell is walked by "
                          "several threads (0: the engine's default, -1: off)")
+    ap.add_argument("--separate-kernels", action="store_true",
+                    help="flat workload: evaluate with the two unfused kernels (a thread per pin event for "
+                         "the dynamic energies, a thread per cell and tile for the leakage), the reference's "
+                         "-disable_fusion baseline, instead of the fused walk")
     ap.add_argument("--no-clock-runs", action="store_true",
                     help="walk periodic clock pins edge by edge instead of as runs of whole cycles")
     ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream", "gemm"],
@@ -789,7 +793,8 @@ def main():
 
     eng = B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                     gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
-                    clock_runs=not args.no_clock_runs, split_events=args.split_events)
+                    clock_runs=not args.no_clock_runs, split_events=args.split_events,
+                    separate_kernels=args.separate_kernels)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     def device_step():
@@ -803,7 +808,9 @@ def main():
 
     # per step: tile_first, glitch_pw, pclk, work_keys (then the library's
     # radix sort), split_count (then the library's scan), the walk (one pin
-    # bucket here), finalize_cells, finalize_cycles
+    # bucket here), finalize_cells, finalize_cycles; with the separate
+    # kernels: tile_first, glitch_pw, sep_net_range, sep_cell_count (then the
+    # library's scan), sep_dyn, power_leak (one pin bucket), the two finalize
     launches_per_step = 8
     from gtpower_b200 import _abi
     import ctypes as C
@@ -879,7 +886,7 @@ def main():
         with B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                        gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
                        clock_runs=not args.no_clock_runs, split_events=args.split_events,
-                       collect_counts=True) as ceng:
+                       separate_kernels=args.separate_kernels, collect_counts=True) as ceng:
             ceng.push_device(n_event, d_off.data_ptr(), d_t.data_ptr(), d_v.data_ptr())
             counts_res = ceng.fetch(counts=True)
 
@@ -905,15 +912,19 @@ def main():
                        "cell_cycles_per_s": world * design.n_cell * eng.n_period / (step_ms / 1e3),
                        "l2": "inputs larger than L2 (event CSR %.2f GB)" % (h2d / 1e9),
                        "walk_ms": walk_ms, "generation_s": gen_s,
-                       "clock_pins": "edge by edge" if args.no_clock_runs else "runs of whole cycles when periodic",
+                       "clock_pins": ("edge by edge" if args.no_clock_runs or args.separate_kernels
+                                      else "runs of whole cycles when periodic"),
+                       "evaluation": ("separate kernels: a thread per pin event (dynamic), then a thread per "
+                                      "cell and tile (leakage)" if args.separate_kernels else "fused walk"),
                        "parallelism": f"weak: {world} independent traces" if world > 1 else "1 GPU"},
             "e2e": {"value": world * n_event / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                     "windows": len(e2e_wins), "split": args.e2e_split if len(e2e_wins) > 1 else "one window"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": None if args.separate_kernels else traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                         "algorithmic_bytes_per_launch": b_alg, "kernel": "power_walk_kernel"},
+                         "algorithmic_bytes_per_launch": b_alg,
+                         "kernel": "sep_dyn_kernel + power_leak_kernel" if args.separate_kernels else "power_walk_kernel"},
             "cpu_baseline": cpu,
             "parity": parity,
             "gpu_launches": launches_per_step * args.steps,

@@ -91,6 +91,8 @@ struct gtp_ctx {
   unsigned long long* d_cyc_acc_g = nullptr;
   float* d_cycle5_g = nullptr;
   unsigned long long* d_leak_tmp_g = nullptr;
+  // the separate dynamic and leakage kernels (cfg.separate_kernels)
+  SeparateScratch sep{};
 };
 
 namespace {
@@ -131,7 +133,8 @@ void free_all(gtp_ctx* c) {
                   c->d_cnt_cell, c->d_cnt_cyc, c->d_status, c->d_cell5, c->d_cycle5, c->d_tg,
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
-                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp, c->d_tiles};
+                  c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp, c->d_tiles,
+                  c->sep.net_lo, c->sep.net_cnt, c->sep.cell_cnt, c->sep.cell_off, c->sep.temp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& sl : c->slot)
@@ -235,6 +238,8 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   // starts at its first tick instead of carrying over
   const bool standalone = ranges != nullptr || (!c->any_window && t_lo > 0) ||
                           (c->any_window && t_lo > c->last_t_hi);
+  // the separate kernels walk every clock edge, in the design's cell order
+  const bool sep = c->cfg.separate_kernels > 0;
 
   KParams k = make_params(c);
   k.net_off = d_net_off;
@@ -329,9 +334,9 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
     }
     if (c->d_glitch_pw) k.glitch_pw = c->d_glitch_pw;
   }
-  const bool sorted = c->cfg.sort_by_work && c->d_order_work && !ranges;
+  const bool sorted = c->cfg.sort_by_work && c->d_order_work && !ranges && !sep;
   if (sorted) k.order = c->d_order_work;
-  if (runs && !standalone) k.pclk = c->d_pclk;
+  if (runs && !standalone && !sep) k.pclk = c->d_pclk;
   if (enqueue_prep) {
     cudaError_t e = cudaSuccess;
     if (k.tile_first) e = launch_tile_first(k, nullptr, c->d_tile_first, stream);
@@ -377,6 +382,11 @@ void commit_window(gtp_ctx* c, int64_t t_hi) {
 gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
                       const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
                       int64_t t_lo, int64_t t_hi, const std::vector<int64_t>* ranges = nullptr) {
+  const bool sep = c->cfg.separate_kernels > 0;
+  if (sep && ranges) {
+    c->err = "separate_kernels: the two-kernel evaluation takes whole windows, not cycle ranges";
+    return GTP_EINVAL;
+  }
   KParams k;
   gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, c->stream, &k, true, ranges);
   if (st != GTP_OK) return st;
@@ -387,6 +397,12 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   const Packed& P = c->P;
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   const bool counts = c->cfg.collect_counts != 0;
+  if (sep) {
+    cudaError_t e = launch_separate_kernels(k, P.bucket_begin, counts, threads, c->sep, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "separate kernels launch");
+    commit_window(c, t_hi);
+    return GTP_OK;
+  }
   // density split: cells whose measured events per tile exceed split_events
   // are walked by several threads, each over part of the tile's cycles
   if (!ranges && c->d_item_off && c->cfg.sort_by_work && c->d_order_work && P.bucket_begin[3] > 0) {
@@ -535,6 +551,15 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
         e = cudaMalloc(&c->d_item_off, sizeof(int32_t) * (nc + 1));
         if (e == cudaSuccess) e = cudaMalloc(&c->d_split_temp, c->split_temp_bytes);
       }
+    }
+    if (e == cudaSuccess && c->cfg.separate_kernels > 0) {
+      c->sep.temp_bytes = std::max<size_t>(1, separate_scan_temp_bytes(P.n_cell));
+      const size_t nn = static_cast<size_t>(std::max<int32_t>(1, P.n_net));
+      e = cudaMalloc(&c->sep.net_lo, sizeof(int64_t) * nn);
+      if (e == cudaSuccess) e = cudaMalloc(&c->sep.net_cnt, sizeof(int64_t) * nn);
+      if (e == cudaSuccess) e = cudaMalloc(&c->sep.cell_cnt, sizeof(int64_t) * (nc + 1));
+      if (e == cudaSuccess) e = cudaMalloc(&c->sep.cell_off, sizeof(int64_t) * (nc + 1));
+      if (e == cudaSuccess) e = cudaMalloc(&c->sep.temp, c->sep.temp_bytes);
     }
     if (e != cudaSuccess) goto cuda_err;
   }
@@ -1062,6 +1087,11 @@ gtp_status gtp_batch_create(gtp_ctx* const* ctxs, int32_t n_ctx, const gtp_batch
   for (int i = 0; i < n_ctx; ++i) {
     gtp_ctx* c = ctxs[i];
     if (!c) return GTP_EINVAL;
+    if (c->cfg.separate_kernels > 0) {
+      set_create_err("gtp_batch_create: the batched walk is the fused one; contexts with separate_kernels are "
+                     "evaluated one window at a time");
+      return GTP_EINVAL;
+    }
     const int t = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
     const int k = c->cfg.collect_counts ? 1 : 0;
     if (i == 0) {
@@ -1395,6 +1425,10 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   }
   if (ev->t_lo != 0 || ev->t_hi <= 0) {
     c->err = "noalloc: evaluates a whole trace; t_lo must be 0 and t_hi > 0";
+    return GTP_EINVAL;
+  }
+  if (c->cfg.separate_kernels > 0) {
+    c->err = "noalloc: the fused walk only; the separate kernels need per-window scratch";
     return GTP_EINVAL;
   }
   int dev = -1;

@@ -288,6 +288,26 @@ cudaError_t compute_split(const unsigned long long* keys_sorted, int32_t n_cell,
                           int64_t n_cyc, int32_t split_events, int32_t* item_off, void* temp, size_t temp_bytes,
                           cudaStream_t stream);
 
+// Scratch of the separate dynamic and leakage kernels (gtp_config.
+// separate_kernels): per net the first evaluated event and their number,
+// per walked cell its pin events and their exclusive prefix, CUB scan
+// temporary storage.
+struct SeparateScratch {
+  int64_t* net_lo;     // [n_net]
+  int64_t* net_cnt;    // [n_net]
+  int64_t* cell_cnt;   // [n_cell + 1]
+  int64_t* cell_off;   // [n_cell + 1]
+  void* temp;
+  size_t temp_bytes;   // separate_scan_temp_bytes(n_cell)
+};
+size_t separate_scan_temp_bytes(int32_t n_cell);
+
+// One window by the two unfused kernels: a thread per pin event for the
+// dynamic energies, then a thread per cell and tile for the leakage, over
+// the walk order p.order[0, bucket_begin[3]) (pin buckets as the walk's).
+cudaError_t launch_separate_kernels(const KParams& p, const int32_t* bucket_begin, bool counts, int threads,
+                                    const SeparateScratch& s, cudaStream_t stream);
+
 // Finalize kernels: per-cell floats, totals/groups, per-cycle floats.
 // With d_cycle5_g (and p.cyc_acc_g), also the per-group per-cycle floats
 // [n_cgroup][5][n_period], using d_leak_tmp_g [n_cgroup][n_period].

@@ -325,9 +325,12 @@ __device__ __forceinline__ float glitch_ratio(const KParams& p, int64_t e, int64
 // One work item of the walk: the cells order[order_begin + gblk * gates_per_block ...]
 // of one pin bucket over cycle tile `tile` of the window, with the block's
 // dynamic shared memory `smem`. All threads of the block call it together.
-template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS, bool RING_EV>
+// DYN = false walks the leakage alone (the leakage kernel of the separate
+// two-kernel evaluation): the merge and the leakage steps, no energies.
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS, bool RING_EV, bool DYN = true>
 __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, const int tile, const int n_blk,
                                            unsigned long long* smem) {
+  static_assert(DYN || (!COUNTS && !RUNS), "the leakage-only walk keeps no counts and walks every edge");
   const int64_t ct = p.cycles_per_tile;
   // per-cycle groups: two bin sets, for the block's first group and the next
   const int nset = p.cell_cgroup ? 2 : 1;
@@ -905,7 +908,7 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
       level_change(cur_abs, cyc, cq, leak_of(ones));
 
       // energies of the triggered pins, in pin order, from the pre-step state
-      uint32_t tb = trig;
+      uint32_t tb = DYN ? trig : 0u;
       while (tb) {
         const int i = __ffs(tb) - 1;
         tb &= tb - 1;
@@ -1363,6 +1366,240 @@ __global__ void pclk_kernel(const KParams pv, const KParams* __restrict__ pd, co
   }
 }
 
+// ---- separate dynamic and leakage kernels (the unfused evaluation) ----
+//
+// The reference's naive baseline (-disable_fusion; GlobalConfig's
+// cuda_power_separate_kernels_for_dyn_and_leak, util/GlobalConfig.hh:28;
+// kernel1_1 / kernel1_2, power/cuda/CudaPower.cu:730-1039): one kernel with
+// a thread per pin event for the dynamic energies, each thread rebuilding
+// the cell's pin state at its event's time by searching every pin's event
+// list, and one with a thread per cell and cycle tile for the leakage (the
+// walk's merge and leakage steps alone, walk_block with DYN = false). The
+// contract, and the integer per-cycle terms, are the fused walk's; the pair
+// is its comparison point.
+
+// Per net: the first listed event in [max(t_lo, 1), min(t_hi, tmax + 1))
+// (the window's events the walk evaluates; tick 0 is the initial
+// condition) and their number. Nets with bad offsets count none (the count
+// kernel reports them).
+__global__ void sep_net_range_kernel(const KParams p, int64_t* __restrict__ net_lo, int64_t* __restrict__ net_cnt) {
+  const int64_t S = max(p.t_lo, static_cast<int64_t>(1));
+  const int64_t E = min(p.t_hi, p.tmax + 1);
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < p.n_net;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = __ldg(p.net_off + n), b = __ldg(p.net_off + n + 1);
+    int64_t lo = a, cnt = 0;
+    if (a >= 0 && b > a && b <= p.n_event && E > S) {
+      lo = lower_bound_time(p.ev_t, a, b, S);
+      cnt = lower_bound_time(p.ev_t, lo, b, E) - lo;
+    }
+    net_lo[n] = lo;
+    net_cnt[n] = cnt;
+  }
+}
+
+// cnt[k] = events of the walked cell at walk-order position k (k < n) over
+// its pins; cnt[n] = 0, so that an exclusive scan ends with the total.
+// Flags what the walk flags per pin: bad offsets, a listing without the
+// event before t_lo, times past time_max.
+__global__ void sep_cell_count_kernel(const KParams p, int32_t n, const int64_t* __restrict__ net_lo,
+                                      const int64_t* __restrict__ net_cnt, int64_t* __restrict__ cnt) {
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= n; k += gridDim.x * blockDim.x) {
+    if (k == n) {
+      cnt[n] = 0;
+      continue;
+    }
+    const int32_t cell = __ldg(p.order + k);
+    const int32_t p0 = __ldg(p.cell_pin_off + cell), p1 = __ldg(p.cell_pin_off + cell + 1);
+    int64_t s = 0;
+    for (int32_t q = p0; q < p1; ++q) {
+      const int32_t net = __ldg(p.pin_net + q);
+      if (net < 0) continue;
+      const int64_t a = __ldg(p.net_off + net), b = __ldg(p.net_off + net + 1);
+      if (a < 0 || b < a || b > p.n_event) {
+        atomicOr(p.status, kErrNetRange);
+        continue;
+      }
+      if (b == a) continue;
+      const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
+      if (base != 0 && __ldg(net_lo + net) == a) atomicOr(p.status, kErrContext);
+      if (ev_time(p.ev_t, b - 1) > p.tmax) atomicOr(p.status, kErrTimeRange);
+      s += __ldg(net_cnt + net);
+    }
+    cnt[k] = s;
+  }
+}
+
+// One thread per pin event g < cell_off[n] (grid-stride): the walk-order
+// position and pin that hold it, the pre-step state of every pin of the
+// cell (a bisection in each pin's events), the related input of an output
+// event, the glitch ratio, the internal and switching energies; per-cell
+// FP64 and per-cycle fixed-point sums by global atomics.
+template <bool COUNTS>
+__global__ void __launch_bounds__(256) sep_dyn_kernel(const KParams p, int32_t n, const int64_t* __restrict__ cell_off,
+                                                      const int64_t* __restrict__ net_lo,
+                                                      const int64_t* __restrict__ net_cnt) {
+  const int64_t total = __ldg(cell_off + n);
+  const int64_t nc = p.n_cell;
+  const int64_t stride = p.n_period + 1;
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    // the last position k with cell_off[k] <= g
+    int32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+      const int32_t m = lo + ((hi - lo) >> 1);
+      if (__ldg(cell_off + m) <= g) lo = m; else hi = m;
+    }
+    const int32_t cell = __ldg(p.order + lo);
+    int64_t r = g - __ldg(cell_off + lo);
+    const int32_t p0 = __ldg(p.cell_pin_off + cell);
+    const DevType ty = p.types[__ldg(p.cell_type + cell)];
+    const int n_pin = ty.n_pin, n_in = ty.n_in;
+    int pin = -1;
+    int64_t e = 0;
+    for (int i = 0; i < n_pin; ++i) {
+      const int32_t net = __ldg(p.pin_net + p0 + i);
+      const int64_t c = net >= 0 ? __ldg(net_cnt + net) : 0;
+      if (r < c) {
+        pin = i;
+        e = __ldg(net_lo + net) + r;
+        break;
+      }
+      r -= c;
+    }
+    if (pin < 0) continue;
+    const int32_t net_i = __ldg(p.pin_net + p0 + pin);
+    const int64_t a_i = __ldg(p.net_off + net_i), b_i = __ldg(p.net_off + net_i + 1);
+    const int64_t cur = ev_time(p.ev_t, e);
+    if (e > a_i && ev_time(p.ev_t, e - 1) >= cur) {
+      atomicOr(p.status, kErrTimeOrder);
+      continue;
+    }
+    const int nv = ev_value(p.ev_v, e);
+    const int pv = e > a_i ? ev_value(p.ev_v, e - 1) : 2;
+    const int tog2 = ntoggle2(pv, nv);
+    const int nr2 = nrise2(pv, nv);
+    const bool rise = nr2 > 0;
+    const int64_t cyc = div_floor_t(cur, p.tpc, p.tpc_magic64);
+    const int64_t cs = cyc * p.tpc;
+    const bool out = pin >= n_in;
+    const int o = pin - n_in;
+    const float* __restrict__ blk = p.inst + __ldg(p.cell_inst + cell);
+    const double cur_s = __dmul_rn(static_cast<double>(cur), p.ts);
+    // pre-step state (events strictly before cur) and the related input:
+    // its last event strictly before cur, in cur's cycle, nearest to cur
+    // less the arc delay
+    uint32_t ones = 0;
+    float best = p.min_diff0;
+    int relq = -1;
+    bool rel_rise = false;
+    for (int j = 0; j < n_pin; ++j) {
+      int v = pv;
+      if (j != pin) {
+        v = __ldg(p.pin_flags + p0 + j) & 3;
+        const int32_t net = __ldg(p.pin_net + p0 + j);
+        if (net >= 0) {
+          const int64_t a = __ldg(p.net_off + net), b = __ldg(p.net_off + net + 1);
+          if (a >= 0 && b > a && b <= p.n_event) {
+            const int64_t pos = lower_bound_time(p.ev_t, a, b, cur);
+            v = pos > a ? ev_value(p.ev_v, pos - 1) : 2;
+            if (out && j < n_in) {
+              const int64_t re = pos > a ? pos - 1 : a;
+              const int64_t tr = ev_time(p.ev_t, re);
+              const bool fr = re > a && nrise2(ev_value(p.ev_v, re - 1), ev_value(p.ev_v, re)) > 0;
+              if (tr >= cs && tr < cs + p.tpc) {
+                const float dl = blk[ty.delay_off + o * n_in * 4 + (rise ? 0 : 1) + j * 4 + (fr ? 0 : 2)];
+                if (!isnan(dl)) {
+                  const double trs = __dmul_rn(static_cast<double>(tr), p.ts);
+                  const float diff = __double2float_rn(fabs(__dsub_rn(__dsub_rn(cur_s, static_cast<double>(dl)), trs)));
+                  if (diff < best) {
+                    best = diff;
+                    relq = j;
+                    rel_rise = fr;
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      if (v == 1) ones |= 1u << j;
+    }
+    // glitch ratio (clock pins never glitch)
+    float gr = -1.0f;
+    if (!(__ldg(p.pin_flags + p0 + pin) & 4)) {
+      const float den = __ldg(p.pin_gden + p0 + pin);
+      if (p.glitch_pw) {
+        gr = glitch_ratio_of(__ldg(p.glitch_pw + e), den);
+      } else {
+        const int64_t base = p.net_base ? __ldg(p.net_base + net_i) : 0;
+        gr = glitch_ratio(p, e, a_i, b_i, base == 0 ? a_i : -1, cur, cs, den);
+      }
+    }
+    // internal energy: the first internal_power group whose `when` holds
+    // (an output's: of its related input, else the default average)
+    float energy = 0.0f;
+    const int32_t s_begin = __ldg(p.pin_slot + ty.pin_slot_off + pin);
+    const int32_t s_end = __ldg(p.pin_slot + ty.pin_slot_off + pin + 1);
+    if (!out) {
+      for (int32_t k = s_begin; k < s_end; ++k) {
+        const DevSlot sl = p.slots[k];
+        if (when_holds(p.cubes, sl.cube_off, sl.n_cube, ones)) {
+          energy = blk[sl.e_off + (rise ? 0 : 1)];
+          break;
+        }
+      }
+    } else if (relq < 0) {
+      energy = blk[ty.def_off + 2 * o + (rise ? 0 : 1)];
+    } else {
+      for (int32_t k = s_begin; k < s_end; ++k) {
+        const DevSlot sl = p.slots[k];
+        if (sl.related != relq) continue;
+        if (when_holds(p.cubes, sl.cube_off, sl.n_cube, ones)) {
+          energy = blk[sl.e_off + (rel_rise ? 0 : 2) + (rise ? 0 : 1)];
+          break;
+        }
+      }
+    }
+    const int64_t cc = cyc < p.n_period ? cyc : p.n_period;
+    const int32_t grp = p.cyc_acc_g ? __ldg(p.cell_cgroup + cell) : 0;
+    auto add = [&](int qc, int qy, float x) {
+      if (x == 0.0f) return;
+      atomicAdd(p.cell_acc + qc * nc + cell, static_cast<double>(x));
+      const unsigned long long f = to_fx_f(x, p.fx_dyn_f, p.fx_dyn);
+      if (f == 0ull) return;
+      atomicAdd(p.cyc_acc + qy * stride + cc, f);
+      if (p.cyc_acc_g) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(grp) * kNumCycAcc + qy) * stride + cc, f);
+    };
+    if (out && nr2 > 0) {
+      // switching: n_rise * C * V^2
+      const float esw = __fmul_rn(nr2 == 2 ? 1.0f : 0.5f, __ldg(p.pin_swe + p0 + pin));
+      if (gr > 0.0f) add(3, kGSw, __fmul_rn(gr, esw));
+      else add(2, kSw, esw);
+    }
+    energy = __fmul_rn(energy, tog2 == 2 ? 1.0f : (tog2 == 1 ? 0.5f : 0.0f));
+    if (gr > 0.0f) add(1, kGInt, __fmul_rn(gr, energy));
+    else add(0, kInt, energy);
+    if (COUNTS) {
+      atomicAdd(p.cnt_cell + 0 * nc + cell, 1u);
+      atomicAdd(p.cnt_cyc + 0 * stride + cc, 1ull);
+      if (gr > 0.0f) {
+        atomicAdd(p.cnt_cell + 1 * nc + cell, 1u);
+        atomicAdd(p.cnt_cyc + 1 * stride + cc, 1ull);
+      }
+      if (tog2) atomicAdd(p.cnt_cell + 2 * nc + cell, static_cast<uint32_t>(tog2));
+      if (out && relq >= 0) atomicAdd(p.cnt_cell + 3 * nc + cell, static_cast<uint32_t>(relq + 1));
+    }
+  }
+}
+
+// The leakage kernel: the walk over cell x tile without the energies.
+template <int MAXP, bool DRIFT>
+__global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_leak_kernel(const __grid_constant__ KParams p) {
+  extern __shared__ unsigned long long smem[];
+  walk_block<MAXP, false, false, DRIFT, false, false, false>(p, blockIdx.x, blockIdx.y, gridDim.x, smem);
+}
+
 // ---- walk order by work ----
 
 __global__ void work_keys_kernel(const KParams p, const int32_t* __restrict__ base_order, int32_t n,
@@ -1708,6 +1945,84 @@ cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int t
                        : launch_t<kMaxPins, false, false, true>(p, threads, stream);
   return counts ? launch_t<kMaxPins, true, false, false>(p, threads, stream)
                 : launch_t<kMaxPins, false, false, false>(p, threads, stream);
+}
+
+namespace {
+template <int MAXP, bool DRIFT>
+cudaError_t launch_leak_t(const KParams& p, int threads, cudaStream_t stream) {
+  const int32_t n = p.order_end - p.order_begin;
+  if (n <= 0) return cudaSuccess;
+  const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, false, threads, 0, 0, p.cell_cgroup ? 2 : 1, false);
+  auto kern = power_leak_kernel<MAXP, DRIFT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  dim3 grid((n + p.gates_per_block - 1) / p.gates_per_block, p.n_tiles);
+  kern<<<grid, threads, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+}  // namespace
+
+size_t separate_scan_temp_bytes(int32_t n_cell) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, static_cast<const int64_t*>(nullptr), static_cast<int64_t*>(nullptr),
+                                static_cast<int64_t>(n_cell) + 1);
+  return b;
+}
+
+cudaError_t launch_separate_kernels(const KParams& p, const int32_t* bucket_begin, bool counts, int threads,
+                                    const SeparateScratch& s, cudaStream_t stream) {
+  const int32_t n = bucket_begin[3];
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  auto blocks_for = [&](int64_t work) -> int {
+    const int64_t b = (work + 255) / 256;
+    return static_cast<int>(b < 1 ? 1 : (b > static_cast<int64_t>(sms) * 16 ? static_cast<int64_t>(sms) * 16 : b));
+  };
+  // 1. per net: the window's events to evaluate
+  if (p.n_net > 0) {
+    sep_net_range_kernel<<<blocks_for(p.n_net), 256, 0, stream>>>(p, s.net_lo, s.net_cnt);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  // 2. per walked cell: its pin events, and their exclusive prefix
+  sep_cell_count_kernel<<<blocks_for(static_cast<int64_t>(n) + 1), 256, 0, stream>>>(p, n, s.net_lo, s.net_cnt,
+                                                                                   s.cell_cnt);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t tb = s.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(s.temp, tb, s.cell_cnt, s.cell_off, static_cast<int64_t>(n) + 1, stream);
+  if (e != cudaSuccess) return e;
+  // 3. the dynamic kernel: a thread per pin event, grid-stride over the
+  // total the scan left on the device
+  {
+    auto kern = counts ? sep_dyn_kernel<true> : sep_dyn_kernel<false>;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, 0);
+    if (e != cudaSuccess) return e;
+    kern<<<sms * (nb > 0 ? nb : 1), 256, 0, stream>>>(p, n, s.cell_off, s.net_lo, s.net_cnt);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  // 4. the leakage kernel: a thread per cell and cycle tile, per pin bucket
+  static const int bucket_pins[3] = {kFastPins, 8, kMaxPins};
+  for (int b = 0; b < 3; ++b) {
+    KParams q = p;
+    q.order_begin = bucket_begin[b];
+    q.order_end = bucket_begin[b + 1];
+    q.item_off = nullptr;
+    q.pclk = nullptr;
+    if (q.order_end <= q.order_begin) continue;
+    const bool d = p.drift != 0;
+    if (bucket_pins[b] == kFastPins) e = d ? launch_leak_t<kFastPins, true>(q, threads, stream)
+                                           : launch_leak_t<kFastPins, false>(q, threads, stream);
+    else if (bucket_pins[b] == 8) e = d ? launch_leak_t<8, true>(q, threads, stream)
+                                        : launch_leak_t<8, false>(q, threads, stream);
+    else e = d ? launch_leak_t<kMaxPins, true>(q, threads, stream) : launch_leak_t<kMaxPins, false>(q, threads, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_finalize(const KParams& p, const uint8_t* cell_group, float* d_cell5,

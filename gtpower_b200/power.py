@@ -88,7 +88,7 @@ class B200Power:
     def __init__(self, design: Design, *, collect_counts: bool = False, device: int = -1,
                  cycles_per_tile: int = 0, threads_per_block: int = 0, gates_per_block: int = 0,
                  max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None,
-                 clock_runs: bool = True, split_events: int = 0):
+                 clock_runs: bool = True, split_events: int = 0, separate_kernels: bool = False):
         self.design = design
         L = _abi.lib()
         cfg = _abi.gtp_config()
@@ -106,6 +106,10 @@ class B200Power:
         # density split: events per thread and tile above which a cell's tile
         # is shared by several threads (0: the default 2048, -1: off)
         cfg.split_events = split_events
+        # the reference's unfused evaluation (-disable_fusion): a kernel with a
+        # thread per pin event for the dynamic energies, then one with a thread
+        # per cell and cycle tile for the leakage
+        cfg.separate_kernels = 1 if separate_kernels else 0
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()

@@ -222,7 +222,19 @@ typedef struct gtp_config {
                                         split_events) threads (at most 32), each
                                         over 1/n of the tile's cycles;
                                         0 = 2048, -1 = off. Needs sort_by_work. */
-  int32_t reserved32;
+  int32_t separate_kernels;          /* 1 = evaluate each window with two separate
+                                        kernels instead of the fused walk, as the
+                                        reference's naive baseline (-disable_fusion,
+                                        GlobalConfig cuda_power_separate_kernels_
+                                        for_dyn_and_leak, util/GlobalConfig.hh:28;
+                                        power/cuda/CudaPower.cu:730-1039): a thread
+                                        per pin event for the dynamic energies, a
+                                        thread per cell and cycle tile for the
+                                        leakage. Same results (per-cycle sums bit
+                                        for bit); a comparison point for the fused
+                                        walk. Not for cycle-range pushes, batches
+                                        or gtp_evaluate_noalloc (GTP_EINVAL).
+                                        0 = fused (default). */
   int64_t reserved[2];
 } gtp_config;
 
