@@ -72,6 +72,9 @@ def parse():
                     help="flat workload: evaluate with the two unfused kernels (a thread per pin event for "
                          "the dynamic energies, a thread per cell and tile for the leakage), the reference's "
                          "-disable_fusion baseline, instead of the fused walk")
+    ap.add_argument("--warp-walk", action="store_true",
+                    help="walk cells of up to 4 pins with one warp each, 32 events at a time (default: one "
+                         "thread per cell and tile)")
     ap.add_argument("--no-clock-runs", action="store_true",
                     help="walk periodic clock pins edge by edge instead of as runs of whole cycles")
     ap.add_argument("--workload", default="flat", choices=["flat", "proxy", "batch", "stream", "gemm"],
@@ -794,7 +797,7 @@ def main():
     eng = B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                     gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
                     clock_runs=not args.no_clock_runs, split_events=args.split_events,
-                    separate_kernels=args.separate_kernels)
+                    separate_kernels=args.separate_kernels, warp_walk=args.warp_walk)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     def device_step():
@@ -886,7 +889,8 @@ def main():
         with B200Power(design, device=local, cycles_per_tile=args.cycles_per_tile,
                        gates_per_block=args.gates_per_block, threads_per_block=args.threads_per_block,
                        clock_runs=not args.no_clock_runs, split_events=args.split_events,
-                       separate_kernels=args.separate_kernels, collect_counts=True) as ceng:
+                       separate_kernels=args.separate_kernels, warp_walk=args.warp_walk,
+                       collect_counts=True) as ceng:
             ceng.push_device(n_event, d_off.data_ptr(), d_t.data_ptr(), d_v.data_ptr())
             counts_res = ceng.fetch(counts=True)
 
@@ -915,7 +919,9 @@ def main():
                        "clock_pins": ("edge by edge" if args.no_clock_runs or args.separate_kernels
                                       else "runs of whole cycles when periodic"),
                        "evaluation": ("separate kernels: a thread per pin event (dynamic), then a thread per "
-                                      "cell and tile (leakage)" if args.separate_kernels else "fused walk"),
+                                      "cell and tile (leakage)" if args.separate_kernels
+                                      else "fused walk, cells of up to 4 pins one warp each" if args.warp_walk
+                                      else "fused walk, one thread per cell and tile"),
                        "parallelism": f"weak: {world} independent traces" if world > 1 else "1 GPU"},
             "e2e": {"value": world * n_event / (e2e_ms / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,

@@ -86,7 +86,7 @@ class gtp_config(C.Structure):
                 ("max_n_pin_for_leakage_power", C.c_int32), ("collect_counts", C.c_int32),
                 ("max_event_num", C.c_int64), ("sort_by_work", C.c_int32),
                 ("clock_runs", C.c_int32), ("split_events", C.c_int32), ("separate_kernels", C.c_int32),
-                ("reserved", C.c_int64 * 2)]
+                ("warp_walk", C.c_int32), ("reserved32", C.c_int32), ("reserved", C.c_int64 * 1)]
 
 
 class gtp_counts(C.Structure):

@@ -419,7 +419,7 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
     k.order_begin = P.bucket_begin[b];
     k.order_end = P.bucket_begin[b + 1];
     if (k.order_end <= k.order_begin) continue;
-    cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, c->stream);
+    cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, c->stream, c->cfg.warp_walk > 0);
     if (e != cudaSuccess) return cuda_fail(c, e, "power walk launch");
   }
   commit_window(c, t_hi);

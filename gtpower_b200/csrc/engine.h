@@ -218,8 +218,10 @@ constexpr int32_t kErrTimeRange = 4;
 constexpr int32_t kErrContext = 8;
 
 // Launches the walk over one bucket of cells. shared-memory bytes computed inside.
+// warp_walk: cells of up to kFastPins pins without drift are walked by one
+// warp each (power_warp_kernel) when the window has its glitch widths.
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
-                              cudaStream_t stream);
+                              cudaStream_t stream, bool warp_walk = false);
 // Persistent walk over many designs' windows (one launch per pin bucket):
 // d_params holds one KParams per (design, bucket), d_items the work items
 // (x: params index, y: gate block, z: tile), *d_n_items their count and

@@ -38,6 +38,9 @@
 #ifndef WALK_MIN_BLOCKS
 #define WALK_MIN_BLOCKS 2   // 2 x 256 threads per SM keeps the walk spill-free
 #endif
+#ifndef WARP_WALK_MIN_BLOCKS
+#define WARP_WALK_MIN_BLOCKS 2
+#endif
 
 namespace gtpb {
 namespace {
@@ -87,6 +90,15 @@ __device__ __forceinline__ int ev_value(const uint32_t* __restrict__ v, int64_t 
 
 __device__ __forceinline__ int64_t ev_time(const int64_t* __restrict__ t, int64_t i) {
   return __ldg(t + i);
+}
+
+// First index in [lo, hi) whose event time is >= x.
+__device__ __forceinline__ int64_t lower_bound_time(const int64_t* __restrict__ t, int64_t lo, int64_t hi, int64_t x) {
+  while (lo < hi) {
+    const int64_t m = lo + ((hi - lo) >> 1);
+    if (ev_time(t, m) < x) lo = m + 1; else hi = m;
+  }
+  return lo;
 }
 
 // getNRise (power/PowerUtils.cc:213-237): returns 2*n_rise (0, 1 or 2).
@@ -164,18 +176,21 @@ constexpr int kInt = 2, kGInt = 3, kSw = 4, kGSw = 5;
 // summed into kInt and kLeakPart when the tile is flushed)
 constexpr int kIntRun = 6, kLeakRun = 7;
 
+// The global-memory side of add_bin: cycles outside the tile's shared bins
+// (kept out of line: rare, and the walks' loops stay small).
+__device__ __noinline__ void add_bin_global(const KParams& p, int32_t g, int q, int64_t c, unsigned long long x) {
+  const int64_t cc = c < 0 ? p.n_period : (c < p.n_period ? c : p.n_period);
+  atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
+  if (p.cyc_acc_g)
+    atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g) * kNumCycAcc + q) * (p.n_period + 1) + cc, x);
+}
+
 __device__ __forceinline__ void add_bin(const KParams& p, const Bins& b, int q, int64_t c,
                                         unsigned long long x) {
   if (x == 0ull) return;
   const int64_t k = c - b.c_lo;
-  if (k >= 0 && k < b.ct && b.off >= 0) {
-    shared_add64(b.s + b.off + q * b.ct + k, x);
-  } else {
-    const int64_t cc = c < 0 ? p.n_period : (c < p.n_period ? c : p.n_period);
-    atomicAdd(p.cyc_acc + q * (p.n_period + 1) + cc, x);
-    if (p.cyc_acc_g)
-      atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(b.g) * kNumCycAcc + q) * (p.n_period + 1) + cc, x);
-  }
+  if (k >= 0 && k < b.ct && b.off >= 0) shared_add64(b.s + b.off + q * b.ct + k, x);
+  else add_bin_global(p, b.g, q, c, x);
 }
 
 // add_bin for cycle c_lo + k of the tile (k >= 0): the shared bin when k < ct
@@ -185,7 +200,7 @@ __device__ __forceinline__ void add_bin_k(const KParams& p, const Bins& b, int q
   if (k < static_cast<uint32_t>(b.ct) && b.off >= 0)
     shared_add64(b.s + b.off + static_cast<uint32_t>(q) * static_cast<uint32_t>(b.ct) + k, x);
   else
-    add_bin(p, b, q, b.c_lo + k, x);
+    add_bin_global(p, b.g, q, b.c_lo + k, x);
 }
 
 __device__ __forceinline__ void add_cnt(const KParams& p, const Bins& b, int q, int64_t c) {
@@ -308,11 +323,16 @@ __device__ float glitch_pw(const KParams& p, int64_t e, int64_t lo, int64_t hi, 
 // Glitch scaling ratio for pulse width pw (s) on a pin whose rise and fall
 // slews sum to den (getTimeBasedGlitchScalingRatioH, PowerUtils.cc:285-294);
 // -1 when pw < 0 (not a glitch event).
+// The reference forms the ratio in double, (pw * 2.0) / den, and rounds it
+// to float; for float operands that equals the correctly rounded float
+// quotient, since double rounding of a quotient through a format of at
+// least 2p + 2 bits is innocuous (53 >= 2 * 24 + 2; S. Figueroa, "When is
+// double rounding innocuous?", SIGNUM Newsletter 30(3), 1995), and pw * 2
+// is exact in float.
 __device__ __forceinline__ float glitch_ratio_of(float pw, float den) {
   if (pw < 0.0f) return -1.0f;
   if (den == 0.0f) return 1.0f;
-  const float r = __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(pw), 2.0),
-                                              static_cast<double>(den)));
+  const float r = __fdiv_rn(__fmul_rn(pw, 2.0f), den);
   return fminf(1.0f, __fmul_rn(r, r));
 }
 
@@ -1127,6 +1147,695 @@ __device__ __forceinline__ void walk_block(const KParams& p, const int gblk, con
   }
 }
 
+// ---- the warp walk: one warp per cell and cycle tile ----
+//
+// Cells of up to kFastPins pins without drift (most of a standard-cell
+// netlist) are walked by one warp each, 32 events at a time in time order,
+// so that the per-event work runs on full lanes instead of one lane per
+// cell. Per chunk of up to 32 events:
+//   - each pin's next 32 events are loaded (coalesced) into a per-warp window
+//     in shared memory as keys (t - T0) << 8 | pin << 5 | slot, which order
+//     events by time, then by pin (same-time events in pin order);
+//   - a merge-path search over the windows gives lane k the cell's k-th
+//     next event;
+//   - the ticks with several events (time groups) come from a ballot; the
+//     pre-step value of each pin for lane k is that of the pin's last event
+//     before k's group (a ballot per pin and a shuffle), else the value
+//     carried from the previous chunk, and so is the related input's last
+//     edge for an output event;
+//   - the leakage level changes once per time group (its last lane), the
+//     energies once per event, with the walk's fixed-point bins and rules;
+//     periodic clock pins are closed as runs by the lanes where the other
+//     pins' state changes.
+// The results are the per-thread walk's (walk_block): the same integer
+// per-cycle terms, per-cell FP64 sums in another order.
+
+constexpr unsigned long long kKeyInf = ~0ull;
+// per-warp window: keys [kFastPins][32], merge scratch [2][32], values [kFastPins][32]
+constexpr int kWarpWinBytes = kFastPins * 32 * 8 + 2 * 32 * 8 + kFastPins * 32;
+
+__device__ __forceinline__ unsigned lanes_below(int k) { return (1u << k) - 1u; }       // k in [0, 31]
+__device__ __forceinline__ unsigned lanes_upto(int k) { return 0xffffffffu >> (31 - k); }  // k in [0, 31]
+
+// Lane k's element of the first 32 of the merge of A[0, 32) and B[0, 32)
+// (ascending, distinct keys, padded with kKeyInf): the split a of the
+// merge path with A[a - 1] < B[k - a] and B[k - a - 1] < A[a].
+__device__ __forceinline__ unsigned long long merge32(const unsigned long long* A, const unsigned long long* B,
+                                                      int k) {
+  int lo = 0, hi = k;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {   // hi - lo <= 31 halves to 0 in 5 steps
+    if (lo < hi) {
+      const int m = (lo + hi) >> 1;
+      if (A[m] < B[k - 1 - m]) lo = m + 1; else hi = m;
+    }
+  }
+  const unsigned long long x = A[lo], y = B[k - lo];
+  return x < y ? x : y;
+}
+
+// Bytes of one warp's shared-memory region: the window, then its copy of
+// the cell's instance block.
+__host__ __device__ __forceinline__ int warp_region_bytes(int inst_stride) {
+  return kWarpWinBytes + ((inst_stride * 4 + 15) / 16) * 16;
+}
+
+// One work item of the warp walk: cells order[order_begin + gblk *
+// gates_per_block ...] (one warp each, in turn) over tile `tile`. All
+// threads of the block call it together.
+template <bool COUNTS, bool RUNS>
+__device__ __forceinline__ void warp_walk_block(const KParams& p, const int gblk, const int tile,
+                                                unsigned long long* smem) {
+  const int64_t ct = p.cycles_per_tile;
+  const int nset = p.cell_cgroup ? 2 : 1;
+  const bool runs_on = RUNS && p.pclk != nullptr;
+  const int nslot = runs_on ? kNumBinSlotsRun : kNumCycAcc;
+  __shared__ unsigned long long s_wsum[32];
+  Bins bins;
+  bins.s = smem;
+  bins.sc = reinterpret_cast<uint32_t*>(smem + nset * nslot * ct);
+  bins.off = 0;
+  bins.g = 0;
+  const int2 tdesc = p.tiles ? p.tiles[tile] : make_int2(0, 0);
+  bins.c_lo = p.tiles ? static_cast<int64_t>(tdesc.x) : p.cyc0 + static_cast<int64_t>(tile) * ct;
+  const int64_t ct_tile = p.tiles ? static_cast<int64_t>(tdesc.y) : ct;
+  bins.ct = ct;
+  for (int64_t k = threadIdx.x; k < nset * nslot * ct; k += blockDim.x) smem[k] = 0ull;
+  if (COUNTS)
+    for (int64_t k = threadIdx.x; k < 2 * ct; k += blockDim.x) bins.sc[k] = 0u;
+  // the per-type tables when they fit, then the warps' regions
+  uint8_t* after_bins = reinterpret_cast<uint8_t*>(smem + nset * nslot * ct + (COUNTS ? ct : 0));
+  const int16_t* fast_tab = p.fast_tab;
+  const float* leak_pool = p.leak_pool;
+  int tab_bytes = 0;
+  if (p.tabs_in_smem) {
+    float* s_leak = reinterpret_cast<float*>(after_bins);
+    int16_t* s_fast = reinterpret_cast<int16_t*>(s_leak + p.n_leak_pool);
+    for (int k = threadIdx.x; k < p.n_leak_pool; k += blockDim.x) s_leak[k] = __ldg(p.leak_pool + k);
+    for (int k = threadIdx.x; k < p.n_fast_tab; k += blockDim.x) s_fast[k] = __ldg(p.fast_tab + k);
+    leak_pool = s_leak;
+    fast_tab = s_fast;
+    tab_bytes = ((p.n_leak_pool * 4 + p.n_fast_tab * 2 + 15) / 16) * 16;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warp = blockDim.x >> 5;
+  uint8_t* wreg = after_bins + tab_bytes + warp * warp_region_bytes(p.fast_inst_stride);
+  unsigned long long* wkey = reinterpret_cast<unsigned long long*>(wreg);   // [kFastPins][32]
+  unsigned long long* wm0 = wkey + kFastPins * 32;                          // [32]
+  unsigned long long* wm1 = wm0 + 32;                                       // [32]
+  uint8_t* wval = reinterpret_cast<uint8_t*>(wm1 + 32);                     // [kFastPins][32]
+  float* winst = reinterpret_cast<float*>(wreg + kWarpWinBytes);
+  __syncthreads();
+
+  // tile window in ticks: [T0, T0 + span)
+  const int64_t T0 = max(p.t_lo, bins.c_lo * p.tpc);
+  const uint32_t off0 = static_cast<uint32_t>(T0 - bins.c_lo * p.tpc);
+  const uint32_t tpc32 = static_cast<uint32_t>(p.tpc);
+  const int64_t t_end = (bins.c_lo + ct_tile) * p.tpc;
+  const int64_t T1 = t_end > p.tmax ? min(p.t_hi, p.tmax + 1) : min(p.t_hi, t_end);
+  const uint32_t span = static_cast<uint32_t>(T1 > T0 ? T1 - T0 : 0);
+  const bool standalone = p.standalone != 0;
+  const bool owns_initial = !standalone && bins.c_lo == 0 && (p.t_lo == 0);
+  const double P = p.period_d;
+  int32_t r_exist = 0;
+  if (runs_on) {
+    const int64_t tl = max(p.t_lo, static_cast<int64_t>(1)) - T0;
+    r_exist = static_cast<int32_t>(max(tl, -static_cast<int64_t>(INT32_MAX / 2)));
+  }
+  const int64_t leak_end = standalone ? min(T0 + static_cast<int64_t>(span), p.tmax) : p.tmax;
+  const bool table_next = p.tile_first && !p.tiles && tile + 1 < p.n_tiles;
+  const int32_t cb0 = p.order_begin + gblk * p.gates_per_block;
+  const int32_t ce0 = min(p.order_end, cb0 + p.gates_per_block);
+  const int32_t g_first = (p.cell_cgroup && cb0 < ce0) ? __ldg(p.cell_cgroup + __ldg(p.order + cb0)) : 0;
+  const unsigned FULL = 0xffffffffu;
+
+  for (int32_t it = cb0 + warp; it < ce0; it += n_warp) {
+    const int32_t cell = __ldg(p.order + it);
+    if (p.cell_cgroup) {
+      bins.g = __ldg(p.cell_cgroup + cell);
+      const int32_t set = bins.g - g_first;
+      bins.off = (set == 0 || set == 1) ? static_cast<int64_t>(set) * nslot * ct : -1;
+    }
+    const int32_t p0 = __ldg(p.cell_pin_off + cell);
+    const int32_t type = __ldg(p.cell_type + cell);
+    const DevType ty = p.types[type];
+    const int n_pin = ty.n_pin, n_in = ty.n_in;
+    const int n_state = 1 << n_pin;
+    const int32_t fo = __ldg(p.type_fast_off + type);
+    {
+      const float* __restrict__ src = p.inst + __ldg(p.cell_inst + cell);
+      for (int k = lane; k < ty.inst_floats; k += 32) winst[k] = __ldg(src + k);
+    }
+    __syncwarp();
+    const float* blk = winst;
+
+    // pin lanes: lane i < n_pin sets up pin i (the walk's per-pin setup)
+    int64_t my_c = 0, my_h = 0;
+    int my_v = 0;
+    int32_t my_lt = kFarBefore;
+    bool my_rise = false, my_atlo = false, my_wave = false, my_clk = false, my_pk = false;
+    int2 my_pc = make_int2(-1, 0);
+    if (lane < n_pin) {
+      const int32_t net = __ldg(p.pin_net + p0 + lane);
+      const uint8_t pf = __ldg(p.pin_flags + p0 + lane);
+      my_v = pf & 3;
+      if (pf & 4) {
+        my_clk = true;
+        if (runs_on && net >= 0 && bins.off >= 0) {
+          my_pc = __ldg(p.pclk + net);
+          my_pk = my_pc.x >= 0;
+        }
+      }
+      if (net >= 0) {
+        const int64_t a = __ldg(p.net_off + net), e = __ldg(p.net_off + net + 1);
+        if (a < 0 || e < a || e > p.n_event) {
+          atomicOr(p.status, kErrNetRange);
+        } else if (e > a) {
+          my_wave = true;
+          const int64_t base = p.net_base ? __ldg(p.net_base + net) : 0;
+          int64_t l = a;
+          if (p.tile_first) {
+            l = a + __ldg(p.tile_first + static_cast<int64_t>(tile) * p.n_net + net);
+          } else {
+            l = lower_bound_time(p.ev_t, a, e, T0);
+          }
+          if (l < e && l == a && base == 0 && ev_time(p.ev_t, l) == 0) ++l;
+          if (l > a) {
+            my_v = ev_value(p.ev_v, l - 1);
+          } else {
+            my_v = 2;
+            if (base != 0) atomicOr(p.status, kErrContext);
+            my_atlo = true;
+          }
+          const int64_t re = l > a ? l - 1 : a;
+          const int64_t pe = re > a ? re - 1 : a;
+          const int64_t tre = ev_time(p.ev_t, re) - T0;
+          my_lt = static_cast<int32_t>(tre < kFarBefore ? kFarBefore : (tre > INT32_MAX / 2 ? INT32_MAX / 2 : tre));
+          my_rise = nrise2(ev_value(p.ev_v, pe), ev_value(p.ev_v, re)) > 0;
+          int64_t h = table_next ? a + __ldg(p.tile_first + static_cast<int64_t>(tile + 1) * p.n_net + net)
+                                 : lower_bound_time(p.ev_t, l, e, T1);
+          if (h < l) h = l;
+          if (h < e && ev_time(p.ev_t, h) > p.tmax) atomicOr(p.status, kErrTimeRange);
+          my_c = l;
+          my_h = h;
+        }
+      }
+    }
+    // the cell's periodic clock pin (at most one, the first): not merged
+    const unsigned pk_cand = __ballot_sync(FULL, my_pk);
+    const int pk = (RUNS && pk_cand) ? __ffs(pk_cand) - 1 : -1;
+    const uint32_t pkbit = (RUNS && pk >= 0) ? (1u << pk) : 0u;
+    const int pc_src = pk >= 0 ? pk : 0;
+    const uint32_t pA = static_cast<uint32_t>(__shfl_sync(FULL, my_pc.x, pc_src));
+    const uint32_t pBv = static_cast<uint32_t>(__shfl_sync(FULL, my_pc.y, pc_src));
+    if (lane == pk) my_h = my_c;
+    const unsigned has_wave = __ballot_sync(FULL, my_wave);
+    const unsigned clock_mask = __ballot_sync(FULL, my_clk);
+    unsigned at_lo = __ballot_sync(FULL, my_atlo);
+    unsigned last_rise = __ballot_sync(FULL, my_rise);
+    // carried 2-bit values of the pins, and the events still to walk
+    uint32_t cst = __reduce_or_sync(FULL, lane < n_pin ? static_cast<uint32_t>(my_v) << (2 * lane) : 0u);
+    uint32_t n_left = __reduce_add_sync(FULL, lane < n_pin ? static_cast<uint32_t>(my_h - my_c) : 0u);
+    // every lane holds each pin's cursor, end and last event time
+    int64_t cur_c[kFastPins], end_h[kFastPins];
+    int32_t last_t[kFastPins];
+#pragma unroll
+    for (int j = 0; j < kFastPins; ++j) {
+      cur_c[j] = __shfl_sync(FULL, my_c, j);
+      end_h[j] = __shfl_sync(FULL, my_h, j);
+      last_t[j] = __shfl_sync(FULL, my_lt, j);
+    }
+    auto ones_of = [&](uint32_t s) -> uint32_t {
+      uint32_t o = 0;
+#pragma unroll
+      for (int j = 0; j < kFastPins; ++j)
+        if (((s >> (2 * j)) & 3u) == 1u) o |= 1u << j;
+      return o;
+    };
+    const float leak_const = ty.leak_const;
+    const int32_t leak_off = ty.leak_off;
+    auto leak_of = [&](uint32_t o) -> float { return leak_off >= 0 ? leak_pool[leak_off + o] : leak_const; };
+    auto in_energy = [&](int i, uint32_t oo, bool rise) -> float {
+      const int16_t eo = fast_tab[fo + i * n_state + oo];
+      return eo >= 0 ? blk[eo + (rise ? 0 : 1)] : 0.0f;
+    };
+    double acc[kNumCellAcc] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    uint32_t n_ev = 0, n_gl = 0, n_half = 0, n_rel = 0;
+    unsigned long long lvl = 0ull;   // fixed-point level this lane added (standalone end)
+    const uint32_t pB = pBv & 0x3fffffffu;
+    const int pv0 = static_cast<int>(pBv >> 31);
+    // clock runs, as the per-thread walk's pclk_jend / pclk_edge / pclk_close
+    auto pclk_jend = [&]() -> uint32_t {
+      const int64_t r_end = ((pBv >> 30) & 1u) ? min(static_cast<int64_t>(span), p.tmax - T0) : static_cast<int64_t>(span);
+      if (r_end <= 0) return 0u;
+      const uint32_t ce = udiv32(static_cast<uint32_t>(r_end - 1) + off0, tpc32, p.tpc_magic);
+      const int32_t he = static_cast<int32_t>(static_cast<uint32_t>(r_end - 1) + off0 - ce * tpc32);
+      return 2 * ce + (he >= static_cast<int32_t>(pA) ? 1u : 0u) + (he >= static_cast<int32_t>(pB) ? 1u : 0u);
+    };
+    auto pclk_edge = [&](uint32_t j, float eA, float eB, float lA, float lB) {
+      const int64_t ce = bins.c_lo + (j >> 1);
+      const int64_t te = T0 + static_cast<int64_t>(static_cast<int32_t>((j >> 1) * tpc32) - static_cast<int32_t>(off0) +
+                                                   static_cast<int32_t>((j & 1) ? pB : pA));
+      const bool ea = !(j & 1);
+      const float en = ea ? eA : eB;
+      acc[0] += en;
+      add_bin_k(p, bins, kInt, j >> 1, to_fx_f(en, p.fx_dyn_f, p.fx_dyn));
+      const double dl = ea ? static_cast<double>(lB) - static_cast<double>(lA)
+                           : static_cast<double>(lA) - static_cast<double>(lB);
+      if (dl != 0.0) {
+        const double cur_s = static_cast<double>(te) * p.ts;
+        const double end_s = fmin(static_cast<double>(ce + 1) * P, p.tmax_s);
+        add_bin_k(p, bins, kLeakPart, j >> 1, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin_k(p, bins, kLeakLevel, (j >> 1) + 1, to_fx(dl * P, p.fx_leak));
+        acc[4] += dl * static_cast<double>(p.tmax - te);
+      }
+      if (COUNTS) {
+        ++n_ev;
+        n_half += 2;
+        add_cnt(p, bins, 0, ce);
+      }
+    };
+    // edges [a, b) under the other pins' state s
+    auto pclk_run = [&](uint32_t a, uint32_t b, uint32_t s) {
+      if (b <= a) return;
+      const uint32_t oA = s | (pv0 ? pkbit : 0u);
+      const uint32_t oB = s | (pv0 ? 0u : pkbit);
+      const float eA = in_energy(pk, oA, pv0 == 0);
+      const float eB = in_energy(pk, oB, pv0 != 0);
+      const float lA = leak_of(oA), lB = leak_of(oB);
+      if (a & 1) pclk_edge(a++, eA, eB, lA, lB);
+      if (b > a && (b & 1)) pclk_edge(--b, eA, eB, lA, lB);
+      if (b > a) {
+        const uint32_t k1 = a >> 1, k2 = b >> 1;
+        const double n = static_cast<double>(k2 - k1);
+        const double dl = static_cast<double>(lB) - static_cast<double>(lA);
+        const unsigned long long e2 = to_fx_f(eA, p.fx_dyn_f, p.fx_dyn) + to_fx_f(eB, p.fx_dyn_f, p.fx_dyn);
+        const unsigned long long l2 = to_fx(dl * (static_cast<double>(pB - pA) * p.ts), p.fx_leak);
+        acc[0] += n * (static_cast<double>(eA) + static_cast<double>(eB));
+        acc[4] += n * dl * static_cast<double>(pB - pA);
+        unsigned long long* run = bins.s + bins.off;
+        if (e2) {
+          shared_add64(run + kIntRun * ct + k1, e2);
+          if (k2 < ct) shared_add64(run + kIntRun * ct + k2, 0ull - e2);
+        }
+        if (l2) {
+          shared_add64(run + kLeakRun * ct + k1, l2);
+          if (k2 < ct) shared_add64(run + kLeakRun * ct + k2, 0ull - l2);
+        }
+        if (COUNTS) {
+          n_ev += 2 * (k2 - k1);
+          n_half += 4 * (k2 - k1);
+          for (uint32_t k = k1; k < k2; ++k) atomicAdd(bins.sc + k, 2u);
+        }
+      }
+    };
+    uint32_t pj = 0;   // next clock edge of the tile not yet accounted
+    if (pkbit) {
+      const uint32_t ph0 = off0 + static_cast<uint32_t>(max(0, r_exist));
+      const uint32_t q0 = udiv32(ph0, tpc32, p.tpc_magic);
+      const uint32_t h0 = ph0 - q0 * tpc32;
+      pj = 2 * q0 + (h0 > pA ? 1u : 0u) + (h0 > pB ? 1u : 0u);
+    }
+    const float leak0 = leak_of(ones_of(cst));
+    if (lane == 0) {
+      if (owns_initial) {
+        acc[4] += static_cast<double>(leak0) * static_cast<double>(p.tmax);
+        add_bin(p, bins, kLeakLevel, 0, to_fx(static_cast<double>(leak0) * P, p.fx_leak));
+      }
+      if (standalone && leak0 != 0.0f) {
+        // the leakage of a standalone part starts at its first tick
+        const uint32_t k0 = udiv32(off0, tpc32, p.tpc_magic);
+        const double dl = static_cast<double>(leak0);
+        const double cur_s = static_cast<double>(T0) * p.ts;
+        const double end_s = fmin(static_cast<double>(bins.c_lo + k0 + 1) * P, p.tmax_s);
+        const unsigned long long lv = to_fx(dl * P, p.fx_leak);
+        add_bin_k(p, bins, kLeakPart, k0, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin_k(p, bins, kLeakLevel, k0 + 1, lv);
+        lvl += lv;
+        acc[4] += dl * static_cast<double>(leak_end - T0);
+      }
+    }
+
+    while (n_left > 0) {
+      // 1. each pin's next 32 events into the window, as ordered keys
+#pragma unroll
+      for (int i = 0; i < kFastPins; ++i) {
+        if (i >= n_pin) break;
+        const int64_t ci = cur_c[i];
+        const int64_t hi_i = end_h[i];
+        const int32_t lt_i = last_t[i];
+        const int64_t idx = ci + lane;
+        unsigned long long kk = kKeyInf;
+        uint8_t vv = 0;
+        int32_t rt = 0;
+        if (idx < hi_i) {
+          rt = static_cast<int32_t>(ev_time(p.ev_t, idx) - T0);
+          kk = (static_cast<unsigned long long>(static_cast<uint32_t>(rt)) << 8) |
+               (static_cast<unsigned long long>(i) << 5) | static_cast<unsigned long long>(lane);
+          vv = static_cast<uint8_t>(ev_value(p.ev_v, idx));
+        }
+        const int32_t rprev = __shfl_up_sync(FULL, rt, 1);
+        if (idx < hi_i && ((lane > 0 && rprev >= rt) || (lane == 0 && !((at_lo >> i) & 1u) && rt <= lt_i)))
+          atomicOr(p.status, kErrTimeOrder);
+        wkey[i * 32 + lane] = kk;
+        wval[i * 32 + lane] = vv;
+      }
+      __syncwarp();
+      // 2. lane k's event: the k-th of the merged windows
+      uint32_t am = 0;
+      for (int i = 0; i < n_pin; ++i)
+        if (wkey[i * 32] != kKeyInf) am |= 1u << i;
+      const int na = __popc(am);
+      if (na == 0) break;
+      const int q0 = __ffs(am) - 1;
+      const uint32_t am1 = am & (am - 1);
+      const int q1 = am1 ? __ffs(am1) - 1 : q0;
+      const uint32_t am2 = am1 & (am1 - 1);
+      const int q2 = am2 ? __ffs(am2) - 1 : q0;
+      const uint32_t am3 = am2 & (am2 - 1);
+      const int q3 = am3 ? __ffs(am3) - 1 : q0;
+      // merge rounds: (q0, q1); then (m0, q2), or (q2, q3) and (m0, m1)
+      unsigned long long K = wkey[q0 * 32 + lane];
+      for (int r = 0; r < na - 1; ++r) {
+        const unsigned long long* A = r == 0 ? wkey + q0 * 32 : (na == 4 && r == 1 ? wkey + q2 * 32 : wm0);
+        const unsigned long long* B = r == 0 ? wkey + q1 * 32 : (na == 4 ? (r == 1 ? wkey + q3 * 32 : wm1) : wkey + q2 * 32);
+        unsigned long long* out = r == na - 2 ? nullptr : (r == 0 ? wm0 : wm1);
+        const unsigned long long v = merge32(A, B, lane);
+        if (out) {
+          out[lane] = v;
+          __syncwarp();
+        } else {
+          K = v;
+        }
+      }
+      const bool valid0 = K != kKeyInf;
+      int n_use = __popc(__ballot_sync(FULL, valid0));   // a prefix of the lanes
+      const uint32_t rel = valid0 ? static_cast<uint32_t>(K >> 8) : 0u;
+      const int pin = valid0 ? static_cast<int>((K >> 5) & 3u) : 0;
+      const int slot = static_cast<int>(K & 31u);
+      // a time group that continues past lane 31 is left to the next chunk
+      if (n_use == 32) {
+        const uint32_t t31 = __shfl_sync(FULL, rel, 31);
+        bool more = false;
+        for (int i = 0; i < n_pin; ++i) {
+          const int ui = __popc(__ballot_sync(FULL, pin == i));
+          if (ui < 32) {
+            const unsigned long long kn = wkey[i * 32 + ui];
+            if (kn != kKeyInf && static_cast<uint32_t>(kn >> 8) == t31) more = true;
+          }
+        }
+        if (more) {
+          const uint32_t rp = __shfl_up_sync(FULL, rel, 1);
+          const unsigned gm = __ballot_sync(FULL, lane == 0 || rel != rp);
+          const int k31 = 31 - __clz(gm);
+          if (k31 > 0) n_use = k31;
+        }
+      }
+      const bool valid = lane < n_use;
+      // 3. time groups: [k0, k1] are the lanes of this lane's tick
+      const uint32_t relp = __shfl_up_sync(FULL, rel, 1);
+      const unsigned gmask = __ballot_sync(FULL, valid && (lane == 0 || rel != relp));
+      const int k0 = valid ? 31 - __clz(gmask & lanes_upto(lane)) : lane;
+      const unsigned gafter = gmask & ~lanes_upto(lane);
+      const int k1 = valid ? (gafter ? __ffs(gafter) - 2 : n_use - 1) : lane;
+      const int nv = valid ? static_cast<int>(wval[pin * 32 + slot]) : 0;
+      // pre-step (before the tick) and post-step (after it) pin values
+      unsigned pm[kFastPins];
+#pragma unroll
+      for (int j = 0; j < kFastPins; ++j) pm[j] = __ballot_sync(FULL, valid && pin == j);
+      uint32_t opre = 0, opost = 0;
+      int pv = 2;
+#pragma unroll
+      for (int j = 0; j < kFastPins; ++j) {
+        const unsigned xj = pm[j] & lanes_below(k0);
+        const unsigned yj = pm[j] & lanes_upto(k1);
+        const int vx = __shfl_sync(FULL, nv, xj ? 31 - __clz(xj) : 0);
+        const int vy = __shfl_sync(FULL, nv, yj ? 31 - __clz(yj) : 0);
+        const int cj = static_cast<int>((cst >> (2 * j)) & 3u);
+        const int vpre = xj ? vx : cj;
+        const int vpost = yj ? vy : cj;
+        if (vpre == 1) opre |= 1u << j;
+        if (vpost == 1) opost |= 1u << j;
+        if (j == pin) pv = vpre;
+      }
+      const int tog2 = ntoggle2(pv, nv);
+      const int nr2 = nrise2(pv, nv);
+      const bool rise = nr2 > 0;
+      // the rise flag an output's related-pin choice reads: false for a pin's
+      // first event after an unknown start
+      const bool first_of_pin = (sel<kFastPins>(pm, pin) & lanes_below(lane)) == 0;
+      const int rflag = (valid && rise && !(((at_lo >> pin) & 1u) && first_of_pin)) ? 1 : 0;
+      // each input's last event strictly before the tick
+      int32_t trq[kFastPins - 1];
+      int frq[kFastPins - 1];
+#pragma unroll
+      for (int q = 0; q < kFastPins - 1; ++q) {
+        const unsigned xq = pm[q] & lanes_below(k0);
+        const int sq = xq ? 31 - __clz(xq) : 0;
+        const int32_t tx = __shfl_sync(FULL, static_cast<int32_t>(rel), sq);
+        const int rx = __shfl_sync(FULL, rflag, sq);
+        trq[q] = xq ? tx : last_t[q];
+        frq[q] = xq ? rx : static_cast<int>((last_rise >> q) & 1u);
+      }
+      const int64_t cpin = sel<kFastPins>(cur_c, pin);
+      const uint32_t cq = udiv32(rel + off0, tpc32, p.tpc_magic);
+      const int64_t cyc = bins.c_lo + cq;
+      const int32_t cs_rel = static_cast<int32_t>(cq * tpc32) - static_cast<int32_t>(off0);
+      const int32_t ce_rel = cs_rel + static_cast<int32_t>(tpc32);
+      const int64_t cur_abs = T0 + static_cast<int64_t>(rel);
+      const int32_t ph = static_cast<int32_t>(rel) - cs_rel;
+      // the periodic clock's value before and after the tick, from its phase
+      uint32_t o_e = opre;   // the energies' pre-step state
+      float l_old, l_new;
+      bool closing = false;
+      uint32_t jhi = 0;
+      if (pkbit) {
+        const bool hb = ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB);
+        const uint32_t cbb = (hb ? pv0 == 0 : pv0 != 0) ? pkbit : 0u;
+        const bool at_end = ((pBv >> 30) & 1u) && cur_abs >= p.tmax;
+        const bool ha = at_end ? (ph > static_cast<int32_t>(pA) && ph <= static_cast<int32_t>(pB))
+                               : (ph >= static_cast<int32_t>(pA) && ph < static_cast<int32_t>(pB));
+        const uint32_t cba = (ha ? pv0 == 0 : pv0 != 0) ? pkbit : 0u;
+        o_e = (opre & ~pkbit) | cbb;
+        l_old = leak_of((opre & ~pkbit) | cba);
+        l_new = leak_of((opost & ~pkbit) | cba);
+        closing = valid && lane == k1 && ((opost ^ opre) & ~pkbit) != 0;
+        jhi = 2 * cq + (ph >= static_cast<int32_t>(pA) ? 1u : 0u) + (ph >= static_cast<int32_t>(pB) ? 1u : 0u);
+        if (at_end) jhi = min(jhi, pclk_jend());
+      } else {
+        l_old = leak_of(opre);
+        l_new = leak_of(opost);
+      }
+      // 4. leakage: the level changes once per tick, at its last lane
+      if (valid && lane == k1 && l_new != l_old) {
+        const double dl = static_cast<double>(l_new) - static_cast<double>(l_old);
+        const double cur_s = static_cast<double>(cur_abs) * p.ts;
+        const double end_s = fmin(static_cast<double>(cyc + 1) * P, p.tmax_s);
+        const unsigned long long lv = to_fx(dl * P, p.fx_leak);
+        add_bin_k(p, bins, kLeakPart, cq, to_fx(dl * (end_s - cur_s), p.fx_leak));
+        add_bin_k(p, bins, kLeakLevel, cq + 1, lv);
+        lvl += lv;
+        acc[4] += dl * static_cast<double>(leak_end - cur_abs);
+      }
+      // the clock's edges up to a tick where the other pins change belong to
+      // the run of their state before it
+      if (pkbit) {
+        const unsigned cm = __ballot_sync(FULL, closing);
+        const unsigned before = cm & lanes_below(lane);
+        const uint32_t jprev = __shfl_sync(FULL, jhi, before ? 31 - __clz(before) : 0);
+        if (closing) pclk_run(before ? jprev : pj, jhi, opre & ~pkbit);
+        if (cm) pj = max(pj, __shfl_sync(FULL, jhi, 31 - __clz(cm)));
+      }
+      // the periodic clock's last edge strictly before the tick, when it lies
+      // in the window (else the last event before the window)
+      int32_t tr_clk = 0;
+      bool fr_clk = false, has_clk = false;
+      if (pkbit) {
+        const uint32_t jb = 2 * cq + (ph > static_cast<int32_t>(pA) ? 1u : 0u) + (ph > static_cast<int32_t>(pB) ? 1u : 0u);
+        if (jb >= 1) {
+          const uint32_t jl = jb - 1;
+          const int32_t te = static_cast<int32_t>((jl >> 1) * tpc32) - static_cast<int32_t>(off0) +
+                             static_cast<int32_t>((jl & 1) ? pB : pA);
+          if (te >= r_exist) {
+            tr_clk = te;
+            fr_clk = (jl & 1) ? (pv0 != 0) : (pv0 == 0);
+            has_clk = true;
+          }
+        }
+      }
+      // 5. energies of every event, from the pre-step state
+      if (valid) {
+        const int64_t ev_idx = cpin + slot;
+        float g = -1.0f;
+        if (!((clock_mask >> pin) & 1u)) g = glitch_ratio_of(__ldg(p.glitch_pw + ev_idx), __ldg(p.pin_gden + p0 + pin));
+        float energy = 0.0f;
+        if (pin < n_in) {
+          energy = in_energy(pin, o_e, rise);
+        } else {
+          const int o = pin - n_in;
+          float best = p.min_diff0;
+          int relq = -1;
+          bool rel_rise = false;
+          const double cur_s = __dmul_rn(static_cast<double>(cur_abs), p.ts);
+          const float* dlp = blk + ty.delay_off + o * n_in * 4 + (rise ? 0 : 1);
+#pragma unroll
+          for (int q = 0; q < kFastPins - 1; ++q) {
+            if (q >= n_in) break;
+            if (!((has_wave >> q) & 1u)) continue;
+            int32_t tr = trq[q];
+            bool fr = frq[q] != 0;
+            if (q == pk && has_clk) {
+              tr = tr_clk;
+              fr = fr_clk;
+            }
+            if (tr < cs_rel || tr >= ce_rel) continue;   // the related edge lies in this cycle
+            const float dl = dlp[q * 4 + (fr ? 0 : 2)];
+            if (isnan(dl)) continue;
+            const double trs = __dmul_rn(static_cast<double>(T0 + tr), p.ts);
+            const float diff = __double2float_rn(fabs(__dsub_rn(__dsub_rn(cur_s, static_cast<double>(dl)), trs)));
+            if (diff < best) {
+              best = diff;
+              relq = q;
+              rel_rise = fr;
+            }
+          }
+          if (relq < 0) {
+            energy = blk[ty.def_off + 2 * o + (rise ? 0 : 1)];
+          } else {
+            const int16_t eo = fast_tab[fo + n_in * n_state + (o * n_in + relq) * n_state + o_e];
+            if (eo >= 0) energy = blk[eo + (rel_rise ? 0 : 2) + (rise ? 0 : 1)];
+          }
+          if (COUNTS) n_rel += static_cast<uint32_t>(relq + 1);
+          if (nr2 > 0) {
+            const float esw = __fmul_rn(nr2 == 2 ? 1.0f : 0.5f, __ldg(p.pin_swe + p0 + pin));
+            if (g > 0.0f) {
+              const float x = __fmul_rn(g, esw);
+              acc[3] += x;
+              add_bin_k(p, bins, kGSw, cq, to_fx_f(x, p.fx_dyn_f, p.fx_dyn));
+            } else {
+              acc[2] += esw;
+              add_bin_k(p, bins, kSw, cq, to_fx_f(esw, p.fx_dyn_f, p.fx_dyn));
+            }
+          }
+        }
+        energy = __fmul_rn(energy, tog2 == 2 ? 1.0f : (tog2 == 1 ? 0.5f : 0.0f));
+        if (g > 0.0f) {
+          const float x = __fmul_rn(g, energy);
+          acc[1] += x;
+          add_bin_k(p, bins, kGInt, cq, to_fx_f(x, p.fx_dyn_f, p.fx_dyn));
+          if (COUNTS) { ++n_gl; add_cnt(p, bins, 1, cyc); }
+        } else {
+          acc[0] += energy;
+          add_bin_k(p, bins, kInt, cq, to_fx_f(energy, p.fx_dyn_f, p.fx_dyn));
+        }
+        if (COUNTS) {
+          ++n_ev;
+          n_half += static_cast<uint32_t>(tog2);
+          add_cnt(p, bins, 0, cyc);
+        }
+      }
+      // 6. carry each pin's last event to the next chunk
+#pragma unroll
+      for (int j = 0; j < kFastPins; ++j) {
+        if (pm[j]) {
+          const int l = 31 - __clz(pm[j]);
+          const int vl = __shfl_sync(FULL, nv, l);
+          const int32_t tl = __shfl_sync(FULL, static_cast<int32_t>(rel), l);
+          const int rl = __shfl_sync(FULL, rflag, l);
+          cst = (cst & ~(3u << (2 * j))) | (static_cast<uint32_t>(vl) << (2 * j));
+          last_rise = (last_rise & ~(1u << j)) | (rl ? (1u << j) : 0u);
+          at_lo &= ~(1u << j);
+          last_t[j] = tl;
+          cur_c[j] += __popc(pm[j]);
+        }
+      }
+      n_left -= static_cast<uint32_t>(n_use);
+      __syncwarp();
+    }
+
+    if (pkbit && lane == 0) pclk_run(pj, pclk_jend(), ones_of(cst) & ~pkbit);
+    // a standalone part ends at its last tick, unless that lies past
+    // time_max: the level it added is taken back integer for integer
+    unsigned long long lvl_all = lvl;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) lvl_all += __shfl_xor_sync(FULL, lvl_all, d);
+    if (standalone && lane == 0 && T0 + static_cast<int64_t>(span) <= p.tmax) {
+      const int64_t t1 = T0 + static_cast<int64_t>(span);
+      const uint32_t k = udiv32(span + off0, tpc32, p.tpc_magic);
+      const uint32_t h = span + off0 - k * tpc32;
+      const int64_t cyc1 = bins.c_lo + k;
+      if (h == 0) {
+        add_bin_k(p, bins, kLeakLevel, k, 0ull - lvl_all);
+      } else {
+        const double cur_s = static_cast<double>(t1) * p.ts;
+        const double end_s = fmin(static_cast<double>(cyc1 + 1) * P, p.tmax_s);
+        const float lf = leak_of(ones_of(cst));
+        add_bin(p, bins, kLeakPart, cyc1, to_fx(-static_cast<double>(lf) * (end_s - cur_s), p.fx_leak));
+        add_bin(p, bins, kLeakLevel, cyc1 + 1, 0ull - lvl_all);
+      }
+    }
+    // the cell's sums for this tile
+    const int64_t nc = p.n_cell;
+#pragma unroll
+    for (int q = 0; q < kNumCellAcc; ++q) {
+      double a = acc[q];
+#pragma unroll
+      for (int d = 16; d >= 1; d >>= 1) a += __shfl_xor_sync(FULL, a, d);
+      if (lane == 0 && a != 0) atomicAdd(p.cell_acc + q * nc + cell, a);
+    }
+    if (COUNTS) {
+      uint32_t c4[4] = {n_ev, n_gl, n_half, n_rel};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t v = __reduce_add_sync(FULL, c4[q]);
+        if (lane == 0 && v) atomicAdd(p.cnt_cell + q * nc + cell, v);
+      }
+    }
+    __syncwarp();   // the window and the instance copy are the next cell's
+  }
+  __syncthreads();
+  // clock runs: run-differences -> per-cycle sums
+  if (runs_on) {
+    for (int set = 0; set < nset; ++set) {
+      block_inclusive_scan(smem + static_cast<int64_t>(set) * nslot * ct + kIntRun * ct, ct, s_wsum);
+      block_inclusive_scan(smem + static_cast<int64_t>(set) * nslot * ct + kLeakRun * ct, ct, s_wsum);
+    }
+  }
+  // flush the tile's per-cycle bins
+  const int64_t stride = p.n_period + 1;
+  for (int64_t k = threadIdx.x; k < ct; k += blockDim.x) {
+    const int64_t c = bins.c_lo + k;
+    const int64_t cc = c < p.n_period ? c : p.n_period;
+#pragma unroll
+    for (int q = 0; q < kNumCycAcc; ++q) {
+      unsigned long long x0 = smem[q * ct + k];
+      unsigned long long x1 = nset == 2 ? smem[(nslot + q) * ct + k] : 0ull;
+      if (runs_on && (q == kInt || q == kLeakPart)) {
+        const int r = q == kInt ? kIntRun : kLeakRun;
+        x0 += smem[r * ct + k];
+        if (nset == 2) x1 += smem[(nslot + r) * ct + k];
+      }
+      if (x0 + x1) atomicAdd(p.cyc_acc + q * stride + cc, x0 + x1);
+      if (p.cyc_acc_g) {
+        if (x0) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g_first) * kNumCycAcc + q) * stride + cc, x0);
+        if (x1) atomicAdd(p.cyc_acc_g + (static_cast<int64_t>(g_first + 1) * kNumCycAcc + q) * stride + cc, x1);
+      }
+    }
+    if (COUNTS) {
+      const uint32_t a = bins.sc[k], b2 = bins.sc[ct + k];
+      if (a) atomicAdd(p.cnt_cyc + 0 * stride + cc, static_cast<unsigned long long>(a));
+      if (b2) atomicAdd(p.cnt_cyc + 1 * stride + cc, static_cast<unsigned long long>(b2));
+    }
+  }
+}
+
+// One window of one design, cells of up to kFastPins pins without drift:
+// block (x, y) walks gate block x over tile y, one warp per cell.
+template <bool COUNTS, bool RUNS>
+__global__ void __launch_bounds__(256, WARP_WALK_MIN_BLOCKS) power_warp_kernel(const __grid_constant__ KParams p) {
+  extern __shared__ unsigned long long smem[];
+  warp_walk_block<COUNTS, RUNS>(p, blockIdx.x, blockIdx.y, smem);
+}
+
 // One window of one design: block (x, y) walks gate block x over tile y.
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
@@ -1292,14 +2001,6 @@ __global__ void glitch_pw_kernel(const KParams pv, const KParams* __restrict__ p
 
 // ---- periodic clock patterns ----
 
-// First index in [lo, hi) whose event time is >= x.
-__device__ __forceinline__ int64_t lower_bound_time(const int64_t* __restrict__ t, int64_t lo, int64_t hi, int64_t x) {
-  while (lo < hi) {
-    const int64_t m = lo + ((hi - lo) >> 1);
-    if (ev_time(t, m) < x) lo = m + 1; else hi = m;
-  }
-  return lo;
-}
 
 // out[nets[w]] = the window's periodic pattern of net nets[w], one block per
 // net: its events in [TL, TH) = [max(t_lo, 1), min(t_hi, tmax + 1)) are edge
@@ -1852,6 +2553,22 @@ cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <bool COUNTS, bool RUNS>
+cudaError_t launch_warp_t(const KParams& p, int threads, cudaStream_t stream) {
+  const int32_t n = p.order_end - p.order_begin;
+  if (n <= 0) return cudaSuccess;
+  size_t tabs = p.tabs_in_smem ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16 : 0;
+  tabs += static_cast<size_t>(threads / 32) * warp_region_bytes(p.fast_inst_stride);
+  const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads, 0, tabs, p.cell_cgroup ? 2 : 1,
+                                            RUNS && p.pclk != nullptr);
+  auto kern = power_warp_kernel<COUNTS, RUNS>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  dim3 grid((n + p.gates_per_block - 1) / p.gates_per_block, p.n_tiles);
+  kern<<<grid, threads, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
 cudaError_t launch_batch_t(const KParams* d_params, const int4* d_items, const int* d_n_items, int* d_counter,
                            int grid, int threads, size_t smem, cudaStream_t stream) {
@@ -1925,8 +2642,12 @@ size_t power_walk_smem_bytes(int64_t cycles_per_tile, bool counts, int threads, 
 }
 
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, bool warp_walk) {
   const bool d = p.drift != 0;
+  if (max_pins <= kFastPins && warp_walk && !d && p.glitch_pw && threads % 32 == 0) {
+    if (p.pclk) return counts ? launch_warp_t<true, true>(p, threads, stream) : launch_warp_t<false, true>(p, threads, stream);
+    return counts ? launch_warp_t<true, false>(p, threads, stream) : launch_warp_t<false, false>(p, threads, stream);
+  }
   if (max_pins <= kFastPins) {
     if (d) return counts ? launch_t<kFastPins, true, true, true>(p, threads, stream)
                          : launch_t<kFastPins, false, true, true>(p, threads, stream);

@@ -88,7 +88,8 @@ class B200Power:
     def __init__(self, design: Design, *, collect_counts: bool = False, device: int = -1,
                  cycles_per_tile: int = 0, threads_per_block: int = 0, gates_per_block: int = 0,
                  max_n_pin_for_leakage_power: int = 16, sort_by_work: bool | None = None,
-                 clock_runs: bool = True, split_events: int = 0, separate_kernels: bool = False):
+                 clock_runs: bool = True, split_events: int = 0, separate_kernels: bool = False,
+                 warp_walk: bool = False):
         self.design = design
         L = _abi.lib()
         cfg = _abi.gtp_config()
@@ -110,6 +111,9 @@ class B200Power:
         # thread per pin event for the dynamic energies, then one with a thread
         # per cell and cycle tile for the leakage
         cfg.separate_kernels = 1 if separate_kernels else 0
+        # cells of up to 4 pins walked by one warp each, 32 events at a time
+        # (default: one thread per cell and tile)
+        cfg.warp_walk = 1 if warp_walk else 0
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()

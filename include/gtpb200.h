@@ -235,7 +235,16 @@ typedef struct gtp_config {
                                         walk. Not for cycle-range pushes, batches
                                         or gtp_evaluate_noalloc (GTP_EINVAL).
                                         0 = fused (default). */
-  int64_t reserved[2];
+  int32_t warp_walk;                 /* 1 = cells of up to 4 pins on a design without
+                                        tick/seconds drift are walked by one warp each,
+                                        32 events at a time in time order (full lanes,
+                                        coalesced event loads; the density split then
+                                        applies to the other cells only). Same results
+                                        (per-cycle sums bit for bit). 0 = one thread per
+                                        cell and tile (default: faster on the traces
+                                        measured). */
+  int32_t reserved32;
+  int64_t reserved[1];
 } gtp_config;
 
 /* Integer counters that must match the oracle bit-exactly. */

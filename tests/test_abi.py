@@ -42,6 +42,8 @@ def test_struct_layout_matches_c_compiler(tmp_path):
         lines.append(f'printf("{n} %zu\\n", sizeof({n}));')
     for f, _ in _abi.gtp_design._fields_:
         lines.append(f'printf("gtp_design.{f} %zu\\n", offsetof(gtp_design, {f}));')
+    for f, _ in _abi.gtp_config._fields_:
+        lines.append(f'printf("gtp_config.{f} %zu\\n", offsetof(gtp_config, {f}));')
     lines.append("return 0;}")
     src.write_text("\n".join(lines))
     exe = tmp_path / "sz"
@@ -52,6 +54,8 @@ def test_struct_layout_matches_c_compiler(tmp_path):
         assert C.sizeof(getattr(_abi, n)) == int(out[n]), n
     for f, _ in _abi.gtp_design._fields_:
         assert getattr(_abi.gtp_design, f).offset == int(out[f"gtp_design.{f}"]), f
+    for f, _ in _abi.gtp_config._fields_:
+        assert getattr(_abi.gtp_config, f).offset == int(out[f"gtp_config.{f}"]), f
 
 
 def _create(design):
