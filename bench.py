@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--e2e-split", default="ramp", choices=["ramp", "even"],
                     help="e2e windows: 'ramp' grows them 1.5x each (a short first copy, then each copy "
                          "hides behind the walk of the window before), 'even' cuts equal windows")
-    ap.add_argument("--e2e-windows", type=int, default=4,
+    ap.add_argument("--e2e-windows", type=int, default=8,
                     help="the e2e leg pushes the trace from pinned host memory as this many windows "
                          "(with their context), so that each window's copy overlaps the previous walk")
     ap.add_argument("--gates-per-block", type=int, default=0)

@@ -269,6 +269,13 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   ct = std::min(ct, max_ct);
   ct = std::max<int64_t>(ct, (n_cyc + 65534) / 65535);  // grid.y limit
   if (ct > max_ct || ct < 1) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
+  // with the default tile, share the window's cycles evenly among its
+  // tiles, so that no tile holds only a few cycles (each tile sets up every
+  // cell once)
+  if (c->cfg.cycles_per_tile <= 0) {
+    const int64_t nt = (n_cyc + ct - 1) / ct;
+    ct = (n_cyc + nt - 1) / nt;
+  }
   k.cycles_per_tile = ct;
   k.n_tiles = static_cast<int32_t>((n_cyc + ct - 1) / ct);
   k.standalone = standalone ? 1 : 0;
