@@ -58,8 +58,10 @@ def parse():
                     help="skip the parity leg (the timed configuration's outputs against the FP64 oracle)")
     ap.add_argument("--cycles-per-tile", type=int, default=0)
     ap.add_argument("--e2e-split", default="ramp", choices=["ramp", "even"],
-                    help="e2e windows: 'ramp' grows them 1.5x each (a short first copy, then each copy "
-                         "hides behind the walk of the window before), 'even' cuts equal windows")
+                    help="e2e windows: 'ramp' grows them by --e2e-ramp each (a short first copy, then each "
+                         "copy hides behind the walk of the window before), 'even' cuts equal windows")
+    ap.add_argument("--e2e-ramp", type=float, default=1.5,
+                    help="growth of each e2e window over the one before (ramp split)")
     ap.add_argument("--e2e-windows", type=int, default=8,
                     help="the e2e leg pushes the trace from pinned host memory as this many windows "
                          "(with their context), so that each window's copy overlaps the previous walk")
@@ -770,7 +772,7 @@ def main():
         if args.e2e_split == "ramp":
             from gtpower_b200 import windows as _windows
             tpc = design.ticks_per_cycle
-            sizes = 1.5 ** np.arange(args.e2e_windows)
+            sizes = args.e2e_ramp ** np.arange(args.e2e_windows)
             cuts = np.concatenate([[0], np.round(np.cumsum(sizes) / sizes.sum() * args.cycles)]).astype(np.int64)
             cuts = np.unique(cuts)
             wins_src = [_windows.make_window(ev, tpc, int(cuts[k]) * tpc,

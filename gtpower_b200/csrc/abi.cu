@@ -571,11 +571,13 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     if (e != cudaSuccess) goto cuda_err;
   }
   // fixed-point scales: one event's energy, and one level change's leakage
-  // over a period, are at most 2^24 units (resolution max|E| * 2^-24 and
-  // max|leak| * period * 2^-24), so that most adds to a shared bin stay
-  // within its low 32-bit word; a 64-bit bin then holds 2^38 of them
-  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 38));
-  c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * std::ldexp(1.0, 38));
+  // over a period, are at most 2^36 units (resolution max|E| * 2^-36 and
+  // max|leak| * period * 2^-36, so that terms scaled down by a small glitch
+  // ratio keep their precision); a 64-bit bin holds 2^27 of the largest. A
+  // shared bin add is one 32-bit atomic, and a second for the high word
+  // when the term reaches 2^32 units or the low word carries
+  c->fx_dyn = fixed_point_scale(std::max(P.max_abs_energy, 1e-30) * std::ldexp(1.0, 26));
+  c->fx_leak = fixed_point_scale(std::max(P.max_abs_leak, 1e-30) * P.period_d * std::ldexp(1.0, 26));
   if (gtp_reset(c) != GTP_OK) { set_err(c->err); free_all(c); delete c; return GTP_ECUDA; }
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) goto cuda_err;
