@@ -68,3 +68,19 @@ def test_metric_names_the_workload_size():
     assert bench.metric_name(200_000, 10_000) == \
         "net events/s (time-based power walk, flat synthetic 200k cells x 10k cycles)"
     assert bench.metric_name(2000, 50) == "net events/s (time-based power walk, flat synthetic 2k cells x 50 cycles)"
+
+
+def test_reference_arm_line_names_the_engine_workload(capsys):
+    """The reference arm's line carries the same metric and config.workload
+    as the engine's line (both built by bench.metric_name / workload_name),
+    times every cell each timed step, and declares zero copies."""
+    import json
+    import bench
+    args = types.SimpleNamespace(cells=400, cycles=30, steps=1, warmup=1)
+    bench.run_reference(args, 0, 1)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.metric_name(400, 30)
+    assert line["config"]["workload"] == bench.workload_name(args)
+    assert "all 400 cells" in line["cpu_baseline"]["sample"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
