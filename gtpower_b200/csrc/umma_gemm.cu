@@ -218,11 +218,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       const uint32_t lane_base = tmem + static_cast<uint32_t>(acc * BN) + (static_cast<uint32_t>(quarter * 32) << 16);
       const uint16_t* mrow = static_cast<const uint16_t*>(ep.mask) + static_cast<int64_t>(row) * ep.ldm;
       float sq = 0.f;
-      for (int c = 0; c < BN; c += 16) {
-        const int nb = n0 + c;
-        if (nb >= N) break;
-        float v[16];
-        tc::tmem_ld16(lane_base + static_cast<uint32_t>(c), v);
+      // one 16-column chunk of this thread's row, from registers
+      auto chunk = [&](float (&v)[16], const int nb) {
         // the chunk's bias: four 16-byte loads when it lies whole and aligned
         float bv[16];
         if (mode & EPI_BIAS) {
@@ -299,6 +296,33 @@ __global__ void __launch_bounds__(THREADS, 1)
             const float s = warp_sum(v[j]);
             if (lane == 0 && nb + j < N) atomicAdd(&ep.colsum[nb + j], s);
           }
+        }
+      };
+      // the forward modes read 64 columns per TMEM round trip (four loads in
+      // flight, one wait); the others 16
+      const bool wide = (mode & (EPI_MSE | EPI_RELU_BWD | EPI_OUT_BF16_T | EPI_COLSUM)) == 0;
+      for (int c = 0; c < BN;) {
+        const int nb = n0 + c;
+        if (nb >= N) break;
+        if (wide && c + 64 <= BN) {
+          uint32_t r[4][16];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tc::tmem_ld16_nowait(lane_base + static_cast<uint32_t>(c + 16 * q), r[q]);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (nb + 16 * q >= N) break;
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[q][j]);
+            chunk(v, nb + 16 * q);
+          }
+          c += 64;
+        } else {
+          float v[16];
+          tc::tmem_ld16(lane_base + static_cast<uint32_t>(c), v);
+          chunk(v, nb);
+          c += 16;
         }
       }
       if (mode & EPI_MSE) {
