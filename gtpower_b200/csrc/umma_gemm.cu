@@ -44,7 +44,11 @@ struct Cfg {
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE = A_BYTES + B_BYTES;
   static constexpr int TILES = STAGES * STAGE;
-  static constexpr int SMEM = 1024 + TILES + SLACK + 256;
+  // per epilogue warp: one 32-row x 64-column BF16 box staged for a TMA
+  // store (128-byte swizzle, 1024-byte aligned), after the barriers
+  static constexpr int STG_OFF = TILES + SLACK + 1024;
+  static constexpr int STG_BYTES = EPI_WARPS * 32 * 128;
+  static constexpr int SMEM = 1024 + STG_OFF + STG_BYTES;
   static constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators: the epilogue of one tile
                                                  // overlaps the MMAs of the next
 };
@@ -81,8 +85,8 @@ __device__ __forceinline__ void load16_bf16(const uint16_t* row, int n, int N, b
 
 template <int BN>
 __global__ void __launch_bounds__(THREADS, 1)
-    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
-                int K, Epilogue ep) {
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ CUtensorMap tmC, int M, int N, int K, Epilogue ep) {
   using C = Cfg<BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -103,6 +107,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (threadIdx.x == 0) {
     tc::tma_prefetch_desc(&tmA);
     tc::tma_prefetch_desc(&tmB);
+    if (ep.tma_store) tc::tma_prefetch_desc(&tmC);
     for (int s = 0; s < STAGES; ++s) {
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
@@ -199,6 +204,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   } else {
     // epilogue warps: warp w reads TMEM lanes (w % 4) * 32 ..., i.e. tile rows
     const int quarter = warp & 3;
+    uint8_t* stg = smem + C::STG_OFF + quarter * (32 * 128);   // this warp's staged box
     int i = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++i) {
       const int acc = i & 1;
@@ -264,7 +270,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
           v[j] = ok ? x : 0.f;
         }
-        if ((mode & EPI_OUT_BF16) && row_ok) {
+        if ((mode & EPI_OUT_BF16) && row_ok && !ep.tma_store) {
           uint16_t* orow = static_cast<uint16_t*>(ep.out) + static_cast<int64_t>(row) * ep.ldo;
           if (nb + 16 <= N) {
             uint4 q0, q1;
@@ -309,6 +315,11 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
           for (int q = 0; q < 4; ++q) tc::tmem_ld16_nowait(lane_base + static_cast<uint32_t>(c + 16 * q), r[q]);
           tc::tmem_wait_ld();
+          if (ep.tma_store) {
+            // the staged box is free once the previous store has read it
+            if (lane == 0) tc::bulk_wait_read();
+            __syncwarp();
+          }
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             if (nb + 16 * q >= N) break;
@@ -316,6 +327,24 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[q][j]);
             chunk(v, nb + 16 * q);
+            if (ep.tma_store) {
+              // this row's 16-byte pieces 2q, 2q + 1 of 8, at their 128-byte
+              // swizzle positions (piece ^ (row & 7))
+              uint8_t* srow = stg + lane * 128;
+              const uint4 q0 = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+              const uint4 q1 =
+                  make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]), pack2(v[14], v[15]));
+              *reinterpret_cast<uint4*>(srow + (((2 * q) ^ (lane & 7)) << 4)) = q0;
+              *reinterpret_cast<uint4*>(srow + (((2 * q + 1) ^ (lane & 7)) << 4)) = q1;
+            }
+          }
+          if (ep.tma_store) {
+            tc::fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0 && m0 + quarter * 32 < M) {   // rows past M are clipped; a box wholly past them is skipped
+              tc::tma_store_2d(&tmC, stg, nb, m0 + quarter * 32);
+              tc::bulk_commit();
+            }
           }
           c += 64;
         } else {
@@ -334,6 +363,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&acc_empty[acc]);
     }
+    // this warp's stores are complete before the CTA ends
+    if (ep.tma_store && lane == 0) tc::bulk_wait_all();
+    __syncwarp();
   }
   tc::tc_fence_before();
   __syncthreads();
@@ -377,8 +409,8 @@ bool make_map(CUtensorMap* map, const Operand& o, int64_t k, int box_rows) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 template <int BN>
-cudaError_t launch(const CUtensorMap& ma, const CUtensorMap& mb, int m, int n, int k, const Epilogue& ep,
-                   cudaStream_t stream) {
+cudaError_t launch(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mc, int m, int n, int k,
+                   const Epilogue& ep, cudaStream_t stream) {
   using C = Cfg<BN>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
@@ -394,7 +426,7 @@ cudaError_t launch(const CUtensorMap& ma, const CUtensorMap& mb, int m, int n, i
   }
   const int64_t tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
   const int grid = static_cast<int>(std::min<int64_t>(tiles, sms));  // persistent: one CTA per SM
-  gemm_kernel<BN><<<grid, THREADS, C::SMEM, stream>>>(ma, mb, m, n, k, ep);
+  gemm_kernel<BN><<<grid, THREADS, C::SMEM, stream>>>(ma, mb, mc, m, n, k, ep);
   return cudaGetLastError();
 }
 
@@ -419,11 +451,24 @@ cudaError_t gemm_bf16_tn(const Operand& a, const Operand& b, int64_t m, int64_t 
   if ((ep.mode & EPI_COLSUM) && ep.colsum == nullptr) return cudaErrorInvalidValue;
   if (bn == 0) bn = n <= 64 ? 64 : (n <= 128 ? 128 : 256);
   if (bn != 64 && bn != 128 && bn != 256) return cudaErrorInvalidValue;
-  CUtensorMap ma, mb;
+  CUtensorMap ma, mb, mc;
   if (!make_map(&ma, a, k, BM) || !make_map(&mb, b, k, bn)) return cudaErrorInvalidValue;
-  if (bn == 64) return launch<64>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
-  if (bn == 128) return launch<128>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
-  return launch<256>(ma, mb, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), ep, stream);
+  // a forward epilogue writing out[] only stores 32 x 64 boxes by TMA
+  Epilogue e2 = ep;
+  e2.tma_store = 0;
+  mc = ma;
+  if ((ep.mode & EPI_OUT_BF16) && !(ep.mode & (EPI_MSE | EPI_RELU_BWD | EPI_OUT_BF16_T | EPI_COLSUM))) {
+    Operand o;
+    o.ptr = ep.out;
+    o.rows = m;
+    o.ld = ep.ldo;
+    if (make_map(&mc, o, n, 32)) e2.tma_store = 1;
+    else mc = ma;
+  }
+  if (bn == 64) return launch<64>(ma, mb, mc, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), e2, stream);
+  if (bn == 128)
+    return launch<128>(ma, mb, mc, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), e2, stream);
+  return launch<256>(ma, mb, mc, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), e2, stream);
 }
 
 }  // namespace umma

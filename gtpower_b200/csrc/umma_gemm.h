@@ -52,6 +52,9 @@ struct Epilogue {
   // skips the loads of its k-th K block (counted over its tiles), so the MMA
   // issuer's wait for them runs out after spin_limit
   int skip_load_block = -1;
+  // set by gemm_bf16_tn: the BF16 output goes out by TMA stores of staged
+  // 32-row x 64-column boxes (forward modes writing out[] only)
+  int tma_store = 0;
 };
 
 // Row-major bf16 matrix [rows, ld] whose first `k` columns are the K extent.

@@ -202,3 +202,29 @@ def test_dense_toggle_bits_of_windows_match_per_window_bits(n_sel):
     assert torch.equal(out[100:5500], ref[100:5500])
     assert bool((out[:100] == 7.0).all()) and bool((out[5500:] == 7.0).all())
     assert float(ref.float().sum()) > 0
+
+
+@pytest.mark.parametrize("I,H,O,n", [(256, 192, 5, 1000), (128, 64, 3, 333), (512, 512, 33, 4100)])
+def test_predict_matches_bf16_fp64_reference(I, H, O, n):
+    """Inference through the BF16 hidden layers (written by TMA stores of
+    staged 32 x 64 boxes): row counts that end inside a tile, hidden widths
+    below, at and above one column tile, against the FP64 network with the
+    same BF16 roundings."""
+    torch = _torch()
+    rng = np.random.default_rng(I + H + n)
+    X, Y = _teacher(rng, n, I, O)
+    with _proxy(I, H, O, 256) as px:
+        xd = torch.from_numpy(X).to("cuda", torch.bfloat16).contiguous()
+        px.set_training_data(xd, torch.from_numpy(Y).cuda().contiguous())
+        mean, std = px.norm()
+        got = px.predict(xd).cpu().numpy().astype(np.float64)
+        P = px.unflatten(px.params_flat())
+    _, _, Ys = mlp_ref.forward_backward(P.__dict__, X.astype(np.float64), np.zeros((n, O)), bf16=True)
+    ref = Ys * std.astype(np.float64) + mean.astype(np.float64)
+    scale = np.abs(ref).max()
+    err = np.abs(got - ref).max()
+    # FP32 vs FP64 accumulation, then BF16 roundings of the hidden layers that
+    # may land on either side: 1e-2 of the largest output
+    assert err <= 1e-2 * scale, (err, scale)
+    # and no row or column out of place: the error is small everywhere
+    assert np.median(np.abs(got - ref)) <= 1e-3 * scale
