@@ -82,6 +82,12 @@ def read_verilog(path: str) -> Module:
     return mod
 
 
+def _spef_name(s: str) -> str:
+    """A SPEF name as the netlist spells it: SPEF escapes '.', '[', ']', '$'
+    and the like with a backslash (dpath\\.a\\[0\\] for dpath.a[0])."""
+    return normalize(re.sub(r"\\(.)", r"\1", s))
+
+
 def read_spef_caps(path: str) -> dict[str, float]:
     """Net name -> total capacitance in farads."""
     caps = {}
@@ -99,13 +105,13 @@ def read_spef_caps(path: str) -> dict[str, float]:
             elif in_map and s.startswith("*") and not s.startswith("*D_NET") and " " in s:
                 k, v = s.split(None, 1)
                 if k[1:].isdigit():
-                    name_map[k] = normalize(v)
+                    name_map[k] = _spef_name(v)
                 else:
                     in_map = False
             if s.startswith("*D_NET"):
                 in_map = False
                 _, ref, cap = s.split()[:3]
-                caps[name_map.get(ref, normalize(ref))] = float(cap) * c_unit
+                caps[name_map.get(ref, _spef_name(ref))] = float(cap) * c_unit
     return caps
 
 
