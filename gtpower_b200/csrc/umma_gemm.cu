@@ -265,10 +265,22 @@ __global__ void __launch_bounds__(THREADS, 1)
               sq += g * g;
             }
             x = g * ep.grad_scale;
-          } else if (ok && (mode & EPI_OUT_F32)) {
-            ep.out_f[static_cast<int64_t>(row) * ep.ldf + n] = x;
           }
           v[j] = ok ? x : 0.f;
+        }
+        // the FP32 output (outside the MSE mode, which stores it above):
+        // four 16-byte stores when the chunk lies whole and aligned
+        if ((mode & EPI_OUT_F32) && !(mode & EPI_MSE) && row_ok) {
+          float* frow = ep.out_f + static_cast<int64_t>(row) * ep.ldf;
+          if (nb + 16 <= N && (reinterpret_cast<uintptr_t>(frow + nb) & 15) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              *reinterpret_cast<float4*>(frow + nb + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (nb + j < N) frow[nb + j] = v[j];
+          }
         }
         if ((mode & EPI_OUT_BF16) && row_ok && !ep.tma_store) {
           uint16_t* orow = static_cast<uint16_t*>(ep.out) + static_cast<int64_t>(row) * ep.ldo;
