@@ -310,6 +310,32 @@ struct Engine {
     uint32_t events = 0, glitches = 0, half_toggles = 0, related = 0;
   };
 
+  // Census of the reference CPU/CUDA divergences: pin events whose CUDA-path
+  // decision (power/cuda/CudaPower.cu:115-315, 317-584) differs from the CPU
+  // path's, counted while the CPU path is walked. The CUDA rules are taken
+  // for one thread over the whole trace (no cycle-chunk seams).
+  struct Census {
+    int64_t pin_events = 0;          // every walked pin event
+    int64_t toggles = 0;             // events that toggle (the CUDA kernel skips the others)
+    int64_t same_tick_state = 0;     // input toggles looked up by the CUDA kernel with the new
+                                     // values of pins that toggled earlier at the same tick
+                                     // (it walks them in event-index order, updating as it goes)
+    int64_t same_tick_energy = 0;    // of those, the ones whose energy differs
+    int64_t first_event_state = 0;   // pins whose net's first event is after t=0: the CPU path
+                                     // walks it from X, the CUDA kernel takes it as the initial
+                                     // state (counted once per pin, compared no further)
+    int64_t glitch_class_diff = 0;   // glitch or not differs (online per-period counters,
+                                     // unflagged neighbours, the t=0 initial event)
+    int64_t glitch_width_diff = 0;   // both glitch, other pulse width
+    int64_t related_diff = 0;        // output toggles with another related input (delay rounded
+                                     // to ticks, same-cycle rule for logic cells only, ties)
+    int64_t no_group_match = 0;      // output toggles with a related input but no matching
+                                     // `when` group: 0 on the CPU, the default average on CUDA
+    int64_t beyond_cuda_cycles = 0;  // toggles in a cycle at or past ceil(time_max / ticks per
+                                     // cycle), which the CUDA kernel never walks
+    int64_t z_events = 0;            // toggles to or from Z, outside the CUDA 3x3 toggle tables
+  };
+
   struct CycleAcc {
     std::vector<Real> leak, internal, g_internal, sw, g_sw;
     std::vector<int64_t> events, glitches;
@@ -351,7 +377,7 @@ struct Engine {
   }
 
   // findTimeBasedAllPower for one instance.
-  void cell(int32_t ci, CellOut& out, CycleAcc& acc) const {
+  void cell(int32_t ci, CellOut& out, CycleAcc& acc, Census* cen = nullptr) const {
     const int32_t p0 = d.cell_pin_off[ci];
     const gtp_cell_type& ty = d.types[d.cell_type[ci]];
     const int n_pin = ty.n_pin, n_in = ty.n_in;
@@ -407,6 +433,16 @@ struct Engine {
     std::vector<int> st = prev_st;
     std::vector<char> trig(n_pin, 0);
     const double norm_dyn = static_cast<double>(tmax) * ts;  // timeMax * timeScale
+    // census: the CUDA kernel's per-pin period counters
+    // (getGlitchScalingRatioClockCycleBasedOnDeviceOnly, CudaPower.cu:270-315)
+    std::vector<int64_t> cu_period(cen ? n_pin : 0, -1), cu_count(cen ? n_pin : 0, 0);
+    const int64_t cuda_cycles = (tmax + tpc - 1) / tpc;   // ceil_div(max_time, ticks), CudaPower.cu:2662
+    const bool is_logic = (d.cell_group ? d.cell_group[ci] : 0) == GTP_GROUP_COMBINATIONAL;
+    std::vector<uint32_t> seq_ones(cen ? n_pin : 0, 0);
+    std::vector<int> order;
+    if (cen)
+      for (int i = 0; i < n_pin; ++i)
+        if (waves[i].n > 0 && waves[i].time(0) != 0) ++cen->first_event_state;
 
     auto slew = [&](int pin, bool rise) -> float {
       return rise ? d.pin_slew_rise[p0 + pin] : d.pin_slew_fall[p0 + pin];
@@ -434,10 +470,36 @@ struct Engine {
 
       const uint32_t ones = onesMask(prev_st);
       const int64_t cyc = cycleOf(cur);
+      if (cen) {
+        // the CUDA kernel's order (triggered pins by event index) and the states each
+        // lookup sees in it
+        order.clear();
+        for (int i = 0; i < n_pin; ++i)
+          if (trig[i] && frontier[i] - 1 > 0) order.push_back(i);
+        std::sort(order.begin(), order.end(), [&](int a, int b) {
+          return waves[a].off + frontier[a] < waves[b].off + frontier[b];
+        });
+        std::vector<int> seq = prev_st;
+        for (int i : order) {
+          seq_ones[i] = onesMask(seq);
+          seq[i] = st[i];
+        }
+      }
       for (int i = 0; i < n_pin; ++i) {
         if (!trig[i]) continue;
         const float n_tog = nToggle(prev_st[i], st[i]);
         const bool rise = isRise(prev_st[i], st[i]);
+        // the CUDA kernel walks this event: it toggles, is not the net's first event (the
+        // initial state there) and lies inside its cycles
+        const bool cu_walk = cen && n_tog != 0.0f && frontier[i] - 1 > 0 && cyc < cuda_cycles;
+        if (cen) {
+          ++cen->pin_events;
+          if (n_tog != 0.0f) {
+            ++cen->toggles;
+            if (cyc >= cuda_cycles) ++cen->beyond_cuda_cycles;
+            if (prev_st[i] == 3 || st[i] == 3) ++cen->z_events;
+          }
+        }
         // getGlitchScalingRatioClockCycleBasedH
         Real g = kInvalidNToggle;
         {
@@ -450,6 +512,33 @@ struct Engine {
             const int64_t w = std::max(pw, nw);
             if (w != kInvalidPulseWidth) g = glitchRatio(w, slew(i, true), slew(i, false));
           }
+        }
+        if (cu_walk && !d.pin_is_clock[p0 + i]) {
+          // the CUDA rule for this event (called for toggling events only)
+          const Wave& w = waves[i];
+          const int64_t e = frontier[i] - 1;
+          const int64_t pc = cycleOf(w.time(e));
+          if (pc == cu_period[i]) ++cu_count[i];
+          else { cu_period[i] = pc; cu_count[i] = 1; }
+          int64_t cpw = kInvalidPulseWidth, cnw = kInvalidPulseWidth;
+          bool cu_none = false;
+          if (e - 1 >= 0 && cycleOf(w.time(e - 1)) == pc) cpw = w.time(e) - w.time(e - 1);
+          if (e + 1 < w.n && cycleOf(w.time(e + 1)) == pc) {
+            if ((e + 2 < w.n && cycleOf(w.time(e + 2)) == pc) || cu_count[i] % 2 == 1) cnw = w.time(e + 1) - w.time(e);
+          } else if (cu_count[i] % 2 == 1) {
+            cu_none = true;
+          }
+          const int64_t cw = cu_none ? kInvalidPulseWidth : std::max(cpw, cnw);
+          // the CPU path's width, or invalid
+          int64_t qw = kInvalidPulseWidth;
+          if (gflags[i][e]) {
+            int64_t pw = kInvalidPulseWidth, nw = kInvalidPulseWidth;
+            if (e - 1 >= 0 && gflags[i][e - 1]) pw = w.time(e) - w.time(e - 1);
+            if (e + 1 < w.n && gflags[i][e + 1]) nw = w.time(e + 1) - w.time(e);
+            qw = std::max(pw, nw);
+          }
+          if ((cw != kInvalidPulseWidth) != (qw != kInvalidPulseWidth)) ++cen->glitch_class_diff;
+          else if (cw != qw) ++cen->glitch_width_diff;
         }
         Real energy = 0;
         int related_code = -1;
@@ -465,6 +554,21 @@ struct Engine {
                 break;
               }
             }
+          }
+          if (cu_walk && seq_ones[i] != ones) {
+            ++cen->same_tick_state;
+            Real alt = 0;
+            if (!std::isinf(s)) {
+              for (int k = 0; k < ty.n_ipwr; ++k) {
+                const gtp_internal_power& gp = d.internal_powers[ty.ipwr_off + k];
+                if (gp.pin != i) continue;
+                if (whenHolds(gp.when, seq_ones[i])) {
+                  alt = groupPower(gp, rise, s, 0.0f);
+                  break;
+                }
+              }
+            }
+            if (alt != energy) ++cen->same_tick_energy;
           }
         } else {
           // findOutputInternalVal
@@ -489,6 +593,35 @@ struct Engine {
               rel_e = re;
             }
           }
+          if (cu_walk) {
+            // the CUDA rule (getOutputPinInternalEnergyVal, CudaPower.cu:172-235)
+            int64_t min_t = tmax;
+            int cu_rel = -1;
+            int64_t cu_e = -1;
+            for (int q = 0; q < n_in; ++q) {
+              const Wave& wq = waves[q];
+              if (wq.n == 0) continue;
+              const int64_t re = std::max<int64_t>(0, lowerBound(wq, cur) - 1);
+              const int64_t pe = std::max<int64_t>(0, re - 1);
+              const bool from_rise = isRise(wq.value(pe), wq.value(re));
+              const float dl = arcs[(static_cast<int64_t>(out_local) * n_in + q) * 4 +
+                                    2 * (from_rise ? 0 : 1) + (rise ? 0 : 1)];
+              if (std::isnan(dl)) continue;
+              const double dt = static_cast<double>(dl) / static_cast<double>(static_cast<float>(ts));
+              const int64_t dtk = static_cast<int64_t>(dt >= 0.0 ? dt + 0.5 : dt - 0.5);
+              const int64_t delta = cur - (wq.time(re) + dtk);
+              const int64_t diff = delta >= 0 ? delta : -delta;
+              if (is_logic && cycleOf(wq.time(re)) != cyc) continue;
+              const int64_t tie = diff >= min_t ? diff - min_t : min_t - diff;
+              const bool near_tie = cu_rel >= 0 && wq.time(re) == waves[cu_rel].time(cu_e) && tie <= 1;
+              if (diff < min_t || (near_tie && re + wq.off > cu_e + waves[cu_rel].off)) {
+                min_t = diff;
+                cu_rel = q;
+                cu_e = re;
+              }
+            }
+            if (cu_rel != rel) ++cen->related_diff;
+          }
           if (rel < 0) {
             // getDefaultOutputPinInternalEnergyVal
             int n_table = 0;
@@ -512,16 +645,19 @@ struct Engine {
             const int64_t pe = std::max<int64_t>(0, rel_e - 1);
             const bool from_rise = isRise(wr.value(pe), wr.value(rel_e));
             const float s = slew(rel, from_rise);
+            bool matched = false;
             if (!std::isinf(s)) {
               for (int k = 0; k < ty.n_ipwr; ++k) {
                 const gtp_internal_power& gp = d.internal_powers[ty.ipwr_off + k];
                 if (gp.pin != i || gp.related_pin != rel) continue;
                 if (whenHolds(gp.when, ones)) {
                   energy = groupPower(gp, rise, s, cap(i));
+                  matched = true;
                   break;
                 }
               }
             }
+            if (cu_walk && !matched) ++cen->no_group_match;
             related_code = rel + 1;
           }
           // switching
@@ -748,6 +884,38 @@ int64_t oracle_cycle_of(int64_t t, double timescale, float clk_period) {
   d.clk_period = clk_period;
   gtp_events ev{};
   return Engine<double>(d, ev, 16).cycleOf(t);
+}
+
+// Divergence census: the Census counters of the FP64 walk over all cells,
+// written to out[0..n_out) in declaration order (pin_events, toggles,
+// same_tick_state, same_tick_energy, first_event_state, glitch_class_diff,
+// glitch_width_diff, related_diff, no_group_match, beyond_cuda_cycles,
+// z_events). Returns the number of counters.
+int oracle_divergence_census(const gtp_design* d, const gtp_events* ev, int n_threads,
+                             int64_t* out, int n_out) {
+  if (!d || !ev) return -2;
+  using Eng = Engine<double>;
+  Eng eng(*d, *ev, 16);
+  if (n_threads < 1) n_threads = 1;
+  constexpr int kN = static_cast<int>(sizeof(Eng::Census) / sizeof(int64_t));
+  std::vector<Eng::Census> cens(n_threads);
+  auto job = [&](int tid) {
+    Eng::CycleAcc acc;
+    acc.init(eng.n_period);
+    for (int32_t ci = tid; ci < d->n_cell; ci += n_threads) {
+      Eng::CellOut o;
+      eng.cell(ci, o, acc, &cens[tid]);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < n_threads; ++t) th.emplace_back(job, t);
+  for (auto& t : th) t.join();
+  for (int k = 0; k < kN && k < n_out; ++k) {
+    int64_t v = 0;
+    for (const auto& c : cens) v += reinterpret_cast<const int64_t*>(&c)[k];
+    out[k] = v;
+  }
+  return kN;
 }
 
 float oracle_n_rise(int prev, int cur) { return nRise(prev, cur); }

@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
         L.oracle_n_toggle.argtypes = [C.c_int, C.c_int]
         L.oracle_glitch_ratio.restype = C.c_double
         L.oracle_glitch_ratio.argtypes = [C.c_int64, C.c_double, C.c_float, C.c_float, C.c_int]
+        L.oracle_divergence_census.restype = C.c_int
+        L.oracle_divergence_census.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -112,6 +114,41 @@ def run(design, events, fp32: bool = False, threads: int = 1, cells: np.ndarray 
     if rc != 0:
         raise RuntimeError(f"oracle_run failed: {rc}")
     return OracleResult(cell5, cyc5, tot, grp, ce, cg, ch, cr, ye, yg, int(dropped[0]), secs.value)
+
+
+CENSUS_FIELDS = ("pin_events", "toggles", "same_tick_state", "same_tick_energy",
+                 "first_event_state", "glitch_class_diff", "glitch_width_diff", "related_diff",
+                 "no_group_match", "beyond_cuda_cycles", "z_events")
+
+
+def divergence_census(design, events, threads: int = 1) -> dict:
+    """Counts the pin events on which the reference's CUDA kernel
+    (power/cuda/CudaPower.cu:317-584) decides differently from its CPU path
+    (power/TimeBasedPower.cc), which this package follows. Keys:
+    pin_events, toggles - every walked pin event, and the toggling ones;
+    same_tick_state, same_tick_energy - input toggles that the CUDA kernel
+    looks up with the new values of pins toggled earlier at the same tick,
+    and those among them whose energy differs; first_event_state - pins
+    whose net's first event is after t=0 (the CUDA kernel takes it as the
+    initial state); glitch_class_diff, glitch_width_diff - toggles that
+    the CUDA per-period counters classify as glitch/non-glitch otherwise,
+    or give another pulse width; related_diff - output toggles with
+    another related input (delays rounded to ticks, the same-cycle rule
+    for combinational cells only, near ties); no_group_match - output
+    toggles with a related input and no matching `when` group (0 on the
+    CPU path, the default average on CUDA); beyond_cuda_cycles - toggles
+    at or past the CUDA kernel's ceil(time_max / ticks per cycle) cycles;
+    z_events - toggles to or from Z. The comparisons cover the events the
+    CUDA kernel walks (toggles after a net's first event, inside its
+    cycles), with one thread over the whole trace."""
+    L = lib()
+    d = design.c_struct()
+    e = events.c_struct()
+    out = np.zeros(len(CENSUS_FIELDS), dtype=np.int64)
+    n = L.oracle_divergence_census(C.byref(d), C.byref(e), threads, _p(out), out.shape[0])
+    if n != len(CENSUS_FIELDS):
+        raise RuntimeError(f"oracle_divergence_census returned {n}")
+    return dict(zip(CENSUS_FIELDS, (int(v) for v in out)))
 
 
 # ---- the reference's own helpers compiled from its sources (oracle/_ref) ----
