@@ -20,6 +20,7 @@ using namespace gtpb;
 
 struct gtp_ctx {
   int device = 0;
+  int sm_count = 0;                   // SMs of the device (0: unknown)
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // created by the context
   gtp_config cfg;
@@ -217,6 +218,44 @@ bool clock_runs_on(const gtp_ctx* c) {
          c->P.tpc < (int64_t(1) << 30);
 }
 
+// Per-tile setup of a cell (first events, initial states, the bin flush), in
+// cycles of walk work.
+constexpr int64_t kTileSetupCycles = 32;
+
+// Tile count for a window of n_cyc cycles, from nt_min (tiles of at most the
+// largest tile) to 3 x nt_min (tiles of at least 64 cycles). The walk of the
+// largest pin bucket launches G gate blocks per tile and R blocks fit on the
+// device at once, so it runs in ceil(G x nt / R) waves of blocks, each about
+// (n_cyc / nt + kTileSetupCycles) cycles long; the count with the shortest
+// such time wins, the smallest on ties. q: the window's walk parameters with
+// the largest tile (its shared memory bounds the occupancy from below).
+int64_t wave_tile_count(const gtp_ctx* c, const KParams& q, int64_t n_cyc, int64_t nt_min) {
+  if (c->sm_count <= 0 || nt_min < 1) return nt_min;
+  static const int bucket_pins[3] = {4, 8, kMaxPins};
+  int b = 0;
+  for (int k = 1; k < 3; ++k)
+    if (c->P.bucket_begin[k + 1] - c->P.bucket_begin[k] > c->P.bucket_begin[b + 1] - c->P.bucket_begin[b]) b = k;
+  const int64_t n_cells = c->P.bucket_begin[b + 1] - c->P.bucket_begin[b];
+  const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
+  const int gpb = c->cfg.gates_per_block > 0 ? c->cfg.gates_per_block : threads;
+  if (n_cells <= 0) return nt_min;
+  const int per_sm = walk_blocks_per_sm_launch(q, bucket_pins[b], c->cfg.collect_counts != 0, threads);
+  if (per_sm <= 0) return nt_min;
+  const int64_t g = (n_cells + gpb - 1) / gpb;
+  const int64_t r = static_cast<int64_t>(per_sm) * c->sm_count;
+  const int64_t nt_max = std::min<int64_t>({3 * nt_min, std::max<int64_t>(nt_min, n_cyc / 64), 65535});
+  int64_t best = nt_min, best_cost = -1;
+  for (int64_t nt = nt_min; nt <= nt_max; ++nt) {
+    const int64_t waves = (g * nt + r - 1) / r;
+    const int64_t cost = waves * ((n_cyc + nt - 1) / nt + kTileSetupCycles);
+    if (best_cost < 0 || cost < best_cost) {
+      best = nt;
+      best_cost = cost;
+    }
+  }
+  return best;
+}
+
 // Validates one window and sets up its walk parameters *out (sorting the
 // walk order by work on `stream` when configured). The context's window
 // state advances only when the walk is enqueued (commit_window).
@@ -271,9 +310,15 @@ gtp_status prepare_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d
   if (ct > max_ct || ct < 1) { c->err = "window spans too many cycles for one launch"; return GTP_EOVERFLOW; }
   // with the default tile, share the window's cycles evenly among its
   // tiles, so that no tile holds only a few cycles (each tile sets up every
-  // cell once)
+  // cell once), and take the tile count whose blocks fill the SMs' waves best
   if (c->cfg.cycles_per_tile <= 0) {
-    const int64_t nt = (n_cyc + ct - 1) / ct;
+    int64_t nt = (n_cyc + ct - 1) / ct;
+    if (!ranges && !sep && c->cfg.warp_walk <= 0) {
+      KParams q = make_params(c);
+      q.cycles_per_tile = ct;
+      q.pclk = (clock_runs_on(c) && !standalone) ? c->d_pclk : nullptr;
+      nt = wave_tile_count(c, q, n_cyc, nt);
+    }
     ct = (n_cyc + nt - 1) / nt;
   }
   k.cycles_per_tile = ct;
@@ -489,6 +534,10 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
     if (e != cudaSuccess) { set_err(std::string("cudaSetDevice: ") + cudaGetErrorString(e)); delete c; return GTP_ECUDA; }
   }
   cudaGetDevice(&c->device);
+  if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    c->sm_count = 0;
+  }
   e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { set_err(std::string("stream: ") + cudaGetErrorString(e)); delete c; return GTP_ECUDA; }
   c->stream = c->own_stream;

@@ -194,7 +194,10 @@ struct KParams {
   // each tile's leakage starts at its first tick and ends at its last
   // instead of carrying over from the windows before
   int32_t standalone;
-  int32_t standalone_pad;
+  // launch order of power_walk_kernel: 0 = block (x, y) is gate block x of
+  // tile y (tile-major); 1 = gate block y of tile x, so that every tile of
+  // the heaviest gate blocks starts first (set by the launch)
+  int32_t gate_major;
   // density split (optional, one-window walk only): item_off[k] = first walk
   // item of the cell at walk-order position k (exclusive prefix over
   // positions of the number of threads that walk it per tile), n_cell + 1
@@ -222,6 +225,9 @@ constexpr int32_t kErrContext = 8;
 // warp each (power_warp_kernel) when the window has its glitch widths.
 cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int threads,
                               cudaStream_t stream, bool warp_walk = false);
+// Blocks per SM of the per-thread walk launch_power_walk would run for p
+// (without warp_walk); 0 when the occupancy query fails.
+int walk_blocks_per_sm_launch(const KParams& p, int max_pins, bool counts, int threads);
 // Persistent walk over many designs' windows (one launch per pin bucket):
 // d_params holds one KParams per (design, bucket), d_items the work items
 // (x: params index, y: gate block, z: tile), *d_n_items their count and

@@ -1836,11 +1836,17 @@ __global__ void __launch_bounds__(256, WARP_WALK_MIN_BLOCKS) power_warp_kernel(c
   warp_walk_block<COUNTS, RUNS>(p, blockIdx.x, blockIdx.y, smem);
 }
 
-// One window of one design: block (x, y) walks gate block x over tile y.
+// One window of one design: block (x, y) walks gate block x over tile y,
+// or with p.gate_major gate block y over tile x. Blocks start in the order of
+// their linear index, and the walk order puts the heaviest cells first: gate
+// major, the launch as a whole runs heaviest first and ends on light blocks.
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
   extern __shared__ unsigned long long smem[];
-  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, gridDim.x, smem);
+  if (p.gate_major)
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.y, blockIdx.x, gridDim.y, smem);
+  else
+    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, gridDim.x, smem);
 }
 
 // Persistent walk over the windows of many designs: each block takes work
@@ -2535,21 +2541,44 @@ __global__ void finalize_cycles(const KParams p, const unsigned long long* __res
 }
 
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
+size_t walk_smem_t(const KParams& p, int threads) {
+  size_t tabs = (FAST && p.tabs_in_smem) ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16 : 0;
+  if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
+  return power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads, (FAST && WALK_USE_RING) ? MAXP : 0, tabs,
+                               p.cell_cgroup ? 2 : 1, RUNS && p.pclk != nullptr) +
+         (RUNS ? walk_runs_acc_bytes(threads) : 0);
+}
+
+// Blocks of this walk variant resident per SM (0 when the query fails).
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
+int occupancy_t(const KParams& p, int threads) {
+  const size_t smem = walk_smem_t<MAXP, COUNTS, FAST, DRIFT, RUNS>(p, threads);
+  auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT, RUNS>;
+  int nb = 0;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
+template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS = false>
 cudaError_t launch_t(const KParams& p, int threads, cudaStream_t stream) {
   const int32_t n = p.order_end - p.order_begin;
   if (n <= 0) return cudaSuccess;
-  size_t tabs = (FAST && p.tabs_in_smem) ? ((static_cast<size_t>(p.n_leak_pool) * 4 + static_cast<size_t>(p.n_fast_tab) * 2 + 15) / 16) * 16 : 0;
-  if (FAST && WALK_STAGE_INST) tabs += static_cast<size_t>(threads) * p.fast_inst_stride * 4;
-  const size_t smem = power_walk_smem_bytes(p.cycles_per_tile, COUNTS, threads,
-                                            (FAST && WALK_USE_RING) ? MAXP : 0, tabs,
-                                            p.cell_cgroup ? 2 : 1, RUNS && p.pclk != nullptr) +
-                      (RUNS ? walk_runs_acc_bytes(threads) : 0);
+  const size_t smem = walk_smem_t<MAXP, COUNTS, FAST, DRIFT, RUNS>(p, threads);
   auto kern = power_walk_kernel<MAXP, COUNTS, FAST, DRIFT, RUNS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  dim3 grid((n + p.gates_per_block - 1) / p.gates_per_block, p.n_tiles);
-  kern<<<grid, threads, smem, stream>>>(p);
+  const int32_t n_gblk = (n + p.gates_per_block - 1) / p.gates_per_block;
+  KParams q = p;
+  // gate major while the gate blocks fit in grid.y
+  q.gate_major = n_gblk <= 65535 ? 1 : 0;
+  dim3 grid = q.gate_major ? dim3(p.n_tiles, n_gblk) : dim3(n_gblk, p.n_tiles);
+  kern<<<grid, threads, smem, stream>>>(q);
   return cudaGetLastError();
 }
 
@@ -2666,6 +2695,26 @@ cudaError_t launch_power_walk(const KParams& p, int max_pins, bool counts, int t
                        : launch_t<kMaxPins, false, false, true>(p, threads, stream);
   return counts ? launch_t<kMaxPins, true, false, false>(p, threads, stream)
                 : launch_t<kMaxPins, false, false, false>(p, threads, stream);
+}
+
+int walk_blocks_per_sm_launch(const KParams& p, int max_pins, bool counts, int threads) {
+  const bool d = p.drift != 0;
+  if (max_pins <= kFastPins) {
+    if (d) return counts ? occupancy_t<kFastPins, true, true, true>(p, threads)
+                         : occupancy_t<kFastPins, false, true, true>(p, threads);
+    if (p.pclk) return counts ? occupancy_t<kFastPins, true, true, false, true>(p, threads)
+                              : occupancy_t<kFastPins, false, true, false, true>(p, threads);
+    return counts ? occupancy_t<kFastPins, true, true, false>(p, threads)
+                  : occupancy_t<kFastPins, false, true, false>(p, threads);
+  }
+  if (max_pins <= 8) {
+    if (d) return counts ? occupancy_t<8, true, false, true>(p, threads) : occupancy_t<8, false, false, true>(p, threads);
+    return counts ? occupancy_t<8, true, false, false>(p, threads) : occupancy_t<8, false, false, false>(p, threads);
+  }
+  if (d) return counts ? occupancy_t<kMaxPins, true, false, true>(p, threads)
+                       : occupancy_t<kMaxPins, false, false, true>(p, threads);
+  return counts ? occupancy_t<kMaxPins, true, false, false>(p, threads)
+                : occupancy_t<kMaxPins, false, false, false>(p, threads);
 }
 
 namespace {

@@ -117,6 +117,8 @@ class B200Power:
         self._cfg = cfg
         self._d = design.c_struct()
         ctx = C.c_void_p()
+        # bound now: at interpreter exit the module globals may be gone before __del__ runs
+        self._destroy = L.gtp_destroy
         _abi.check(L.gtp_create(C.byref(self._d), C.byref(cfg), C.byref(ctx)))
         self.ctx = ctx
         self.n_period = int(L.gtp_n_period(ctx))
@@ -125,7 +127,7 @@ class B200Power:
 
     def close(self) -> None:
         if getattr(self, "ctx", None):
-            _abi.lib().gtp_destroy(self.ctx)
+            self._destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):

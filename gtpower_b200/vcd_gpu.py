@@ -67,6 +67,8 @@ class GpuVcdReader:
         self._keep = (chars, off, src_id, src_bit)
         self.h = None
         h = C.c_void_p()
+        # bound now: at interpreter exit the module globals may be gone before __del__ runs
+        self._destroy = _abi.lib().gtp_vcd_destroy
         st = _abi.lib().gtp_vcd_create(chars, off.ctypes.data_as(C.c_void_p), len(ids),
                                        src_id.ctypes.data_as(C.c_void_p), src_bit.ctypes.data_as(C.c_void_p),
                                        self.n_src, device, C.byref(h))
@@ -92,7 +94,7 @@ class GpuVcdReader:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            _abi.lib().gtp_vcd_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):
