@@ -60,9 +60,9 @@ def parse():
     ap.add_argument("--e2e-split", default="ramp", choices=["ramp", "even"],
                     help="e2e windows: 'ramp' grows them by --e2e-ramp each (a short first copy, then each "
                          "copy hides behind the walk of the window before), 'even' cuts equal windows")
-    ap.add_argument("--e2e-ramp", type=float, default=1.5,
+    ap.add_argument("--e2e-ramp", type=float, default=1.25,
                     help="growth of each e2e window over the one before (ramp split)")
-    ap.add_argument("--e2e-windows", type=int, default=8,
+    ap.add_argument("--e2e-windows", type=int, default=12,
                     help="the e2e leg pushes the trace from pinned host memory as this many windows "
                          "(with their context), so that each window's copy overlaps the previous walk")
     ap.add_argument("--gates-per-block", type=int, default=0)

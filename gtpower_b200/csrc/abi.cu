@@ -56,7 +56,9 @@ struct gtp_ctx {
   size_t split_temp_bytes = 0;
   // events (host-pushed windows)
   // events pushed from host memory: two device slots, filled on copy_stream
-  // while the walk of the other slot's window runs on `stream`
+  // while the walk of the other slot's window runs; slot s's windows walk on
+  // walk_stream[s], so the next window's walk may start while this one's
+  // last blocks finish
   struct Slot {
     int64_t cap = 0;
     int64_t *d_net_off = nullptr, *d_ev_t = nullptr, *d_net_base = nullptr;
@@ -67,6 +69,31 @@ struct gtp_ctx {
   int next_slot = 0;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copied_ev = nullptr;
+  cudaStream_t walk_stream[2] = {nullptr, nullptr};
+  cudaEvent_t walk_done[2] = {nullptr, nullptr};  // the last walk enqueued on walk_stream[s]
+  bool walk_pending[2] = {false, false};
+  cudaEvent_t stream_tail = nullptr;               // `stream`'s work before a host-pushed walk
+  // the context queued work of its own on `stream` (a reset, a device-pushed
+  // window, a finalize, ...) that the walk streams have not been ordered after
+  bool stream_dirty = true;
+  // per-window walk scratch of the other event slot: the first-event table,
+  // glitch widths, clock patterns, work order and split offsets of the
+  // window that walks on the other stream. The context's own fields hold the
+  // set of slot scratch_slot; swap_scratch exchanges the two.
+  struct WalkScratch {
+    int32_t* tile_first = nullptr;
+    int64_t tile_first_cap = 0;
+    float* glitch_pw = nullptr;
+    int64_t glitch_pw_cap = 0;
+    int2* pclk = nullptr;
+    unsigned long long *keys_in = nullptr, *keys_out = nullptr;
+    int32_t* order_work = nullptr;
+    void* sort_temp = nullptr;
+    int32_t* item_off = nullptr;
+    void* split_temp = nullptr;
+    bool ready = false;
+  } spare;
+  int scratch_slot = 0;
   // accumulators and outputs
   double* d_cell_acc = nullptr;
   unsigned long long* d_cyc_acc = nullptr;
@@ -135,14 +162,78 @@ void free_all(gtp_ctx* c) {
                   c->d_leak_tmp, c->d_type_fast_off, c->d_fast_tab, c->d_keys_in,
                   c->d_keys_out, c->d_order_work, c->d_sort_temp, c->d_cgroup, c->d_cyc_acc_g, c->d_tile_first, c->d_glitch_pw,
                   c->d_cycle5_g, c->d_leak_tmp_g, c->d_clk_nets, c->d_pclk, c->d_item_off, c->d_split_temp, c->d_tiles,
-                  c->sep.net_lo, c->sep.net_cnt, c->sep.cell_cnt, c->sep.cell_off, c->sep.temp};
+                  c->sep.net_lo, c->sep.net_cnt, c->sep.cell_cnt, c->sep.cell_off, c->sep.temp,
+                  c->spare.tile_first, c->spare.glitch_pw, c->spare.pclk, c->spare.keys_in, c->spare.keys_out,
+                  c->spare.order_work, c->spare.sort_temp, c->spare.item_off, c->spare.split_temp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (int k = 0; k < 2; ++k) {
+    if (c->walk_done[k]) cudaEventDestroy(c->walk_done[k]);
+    if (c->walk_stream[k]) cudaStreamDestroy(c->walk_stream[k]);
+  }
+  if (c->stream_tail) cudaEventDestroy(c->stream_tail);
   for (auto& sl : c->slot)
     if (sl.free_ev) cudaEventDestroy(sl.free_ev);
   if (c->copied_ev) cudaEventDestroy(c->copied_ev);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
+}
+
+// Makes stream s wait for the walks of host-pushed windows still in flight
+// on the walk streams.
+cudaError_t join_walks(gtp_ctx* c, cudaStream_t s) {
+  // the caller queues work on s next
+  if (s == c->stream) c->stream_dirty = true;
+  for (int k = 0; k < 2; ++k)
+    if (c->walk_pending[k]) {
+      cudaError_t e = cudaStreamWaitEvent(s, c->walk_done[k], 0);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+void swap_scratch(gtp_ctx* c) {
+  auto& w = c->spare;
+  std::swap(c->d_tile_first, w.tile_first);
+  std::swap(c->tile_first_cap, w.tile_first_cap);
+  std::swap(c->d_glitch_pw, w.glitch_pw);
+  std::swap(c->glitch_pw_cap, w.glitch_pw_cap);
+  std::swap(c->d_pclk, w.pclk);
+  std::swap(c->d_keys_in, w.keys_in);
+  std::swap(c->d_keys_out, w.keys_out);
+  std::swap(c->d_order_work, w.order_work);
+  std::swap(c->d_sort_temp, w.sort_temp);
+  std::swap(c->d_item_off, w.item_off);
+  std::swap(c->d_split_temp, w.split_temp);
+  c->scratch_slot ^= 1;
+}
+
+// Allocates the second scratch set like the first (the tables that grow
+// with the window start empty), on first use.
+cudaError_t ready_spare(gtp_ctx* c) {
+  auto& w = c->spare;
+  if (w.ready) return cudaSuccess;
+  const size_t nc = std::max<int32_t>(1, c->P.n_cell);
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](auto** p, size_t bytes) {
+    if (e == cudaSuccess && !*p) e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+  };
+  if (c->d_pclk) {
+    alloc(&w.pclk, sizeof(int2) * static_cast<size_t>(c->P.n_net));
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.pclk, 0xff, sizeof(int2) * static_cast<size_t>(c->P.n_net), c->stream);
+  }
+  if (c->d_keys_in) {
+    alloc(&w.keys_in, sizeof(unsigned long long) * nc);
+    alloc(&w.keys_out, sizeof(unsigned long long) * nc);
+    alloc(&w.order_work, sizeof(int32_t) * nc);
+    alloc(&w.sort_temp, c->sort_temp_bytes);
+  }
+  if (c->d_item_off) {
+    alloc(&w.item_off, sizeof(int32_t) * (nc + 1));
+    alloc(&w.split_temp, c->split_temp_bytes);
+  }
+  if (e == cudaSuccess) w.ready = true;
+  return e;
 }
 
 KParams make_params(gtp_ctx* c) {
@@ -431,16 +522,20 @@ void commit_window(gtp_ctx* c, int64_t t_hi) {
   c->last_t_hi = t_hi;
 }
 
+// ws: the stream the window's preparation and walk go on (the context's
+// stream, or a walk stream for host-pushed windows).
 gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
                       const uint32_t* d_v, const int64_t* d_base, int64_t n_event,
-                      int64_t t_lo, int64_t t_hi, const std::vector<int64_t>* ranges = nullptr) {
+                      int64_t t_lo, int64_t t_hi, const std::vector<int64_t>* ranges = nullptr,
+                      cudaStream_t ws = nullptr) {
+  if (!ws) ws = c->stream;
   const bool sep = c->cfg.separate_kernels > 0;
   if (sep && ranges) {
     c->err = "separate_kernels: the two-kernel evaluation takes whole windows, not cycle ranges";
     return GTP_EINVAL;
   }
   KParams k;
-  gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, c->stream, &k, true, ranges);
+  gtp_status st = prepare_window(c, d_net_off, d_t, d_v, d_base, n_event, t_lo, t_hi, ws, &k, true, ranges);
   if (st != GTP_OK) return st;
   if (k.n_tiles <= 0) {  // cycle ranges outside the window: nothing to walk
     commit_window(c, t_hi);
@@ -450,7 +545,7 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
   const int threads = c->cfg.n_thread_per_block > 0 ? c->cfg.n_thread_per_block : 256;
   const bool counts = c->cfg.collect_counts != 0;
   if (sep) {
-    cudaError_t e = launch_separate_kernels(k, P.bucket_begin, counts, threads, c->sep, c->stream);
+    cudaError_t e = launch_separate_kernels(k, P.bucket_begin, counts, threads, c->sep, ws);
     if (e != cudaSuccess) return cuda_fail(c, e, "separate kernels launch");
     commit_window(c, t_hi);
     return GTP_OK;
@@ -462,7 +557,7 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
     const int64_t last_tick = std::min<int64_t>(k.t_hi - 1, k.tmax);
     const int64_t n_cyc = std::max<int64_t>(1, last_tick / k.tpc + 1 - k.cyc0);
     cudaError_t e = compute_split(c->d_keys_out, P.bucket_begin[3], k.cycles_per_tile, n_cyc, se, c->d_item_off,
-                                  c->d_split_temp, c->split_temp_bytes, c->stream);
+                                  c->d_split_temp, c->split_temp_bytes, ws);
     if (e != cudaSuccess) return cuda_fail(c, e, "density split");
     k.item_off = c->d_item_off;
   }
@@ -471,7 +566,7 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
     k.order_begin = P.bucket_begin[b];
     k.order_end = P.bucket_begin[b + 1];
     if (k.order_end <= k.order_begin) continue;
-    cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, c->stream, c->cfg.warp_walk > 0);
+    cudaError_t e = launch_power_walk(k, bucket_pins[b], counts, threads, ws, c->cfg.warp_walk > 0);
     if (e != cudaSuccess) return cuda_fail(c, e, "power walk launch");
   }
   commit_window(c, t_hi);
@@ -480,7 +575,8 @@ gtp_status run_window(gtp_ctx* c, const int64_t* d_net_off, const int64_t* d_t,
 
 gtp_status check_status(gtp_ctx* c) {
   int32_t st = 0;
-  cudaError_t e = cudaMemcpyAsync(&st, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&st, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "status read");
   if (st) {
@@ -641,6 +737,8 @@ cuda_err:
 
 void gtp_destroy(gtp_ctx* c) {
   if (!c) return;
+  for (int k = 0; k < 2; ++k)
+    if (c->walk_stream[k]) cudaStreamSynchronize(c->walk_stream[k]);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
   delete c;
@@ -659,7 +757,8 @@ gtp_status gtp_reset(gtp_ctx* c) {
   if (!c) return GTP_EINVAL;
   const size_t nc = std::max<int32_t>(1, c->P.n_cell);
   const size_t ny = static_cast<size_t>(c->P.n_period + 1);
-  cudaError_t e = cudaMemsetAsync(c->d_cell_acc, 0, sizeof(double) * kNumCellAcc * nc, c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cell_acc, 0, sizeof(double) * kNumCellAcc * nc, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cyc_acc, 0, sizeof(unsigned long long) * kNumCycAcc * ny, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cell, 0, sizeof(uint32_t) * 4 * nc, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cnt_cyc, 0, sizeof(unsigned long long) * 2 * ny, c->stream);
@@ -693,9 +792,15 @@ gtp_status gtp_push_events(gtp_ctx* c, const gtp_events* ev) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->copied_ev, cudaEventDisableTiming);
     for (auto& sl : c->slot)
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.free_ev, cudaEventDisableTiming);
+    for (int k = 0; k < 2; ++k) {
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->walk_stream[k], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->walk_done[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->stream_tail, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(c, e, "copy stream");
   }
-  auto& sl = c->slot[c->next_slot];
+  const int s_idx = c->next_slot;
+  auto& sl = c->slot[s_idx];
   // the walk that last read this slot must be done before it is overwritten
   if (sl.used) {
     e = cudaStreamWaitEvent(c->copy_stream, sl.free_ev, 0);
@@ -738,12 +843,39 @@ gtp_status gtp_push_events(gtp_ctx* c, const gtp_events* ev) {
   // the caller's memory is no longer read once this returns; the walk of the
   // previous window keeps running meanwhile
   if (e == cudaSuccess) e = cudaEventSynchronize(c->copied_ev);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->copied_ev, 0);
+  if (e != cudaSuccess) return cuda_fail(c, e, "event copy");
+  // the window walks on its slot's stream with its slot's scratch, after the
+  // copy and after the work enqueued on the context's stream so far (a reset,
+  // device-pushed windows); the separate kernels keep the context's stream
+  cudaStream_t ws = c->stream;
+  if (c->cfg.separate_kernels <= 0) {
+    ws = c->walk_stream[s_idx];
+    if (c->scratch_slot != s_idx) {
+      if (!c->spare.ready) c->stream_dirty = true;  // ready_spare clears on the context's stream
+      e = ready_spare(c);
+      if (e != cudaSuccess) return cuda_fail(c, e, "walk scratch");
+      swap_scratch(c);
+    }
+    // both walk streams follow the context's own work queued so far
+    if (c->stream_dirty) {
+      e = cudaEventRecord(c->stream_tail, c->stream);
+      for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(c->walk_stream[k], c->stream_tail, 0);
+      if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
+      c->stream_dirty = false;
+    }
+  }
+  e = cudaStreamWaitEvent(ws, c->copied_ev, 0);
   if (e != cudaSuccess) return cuda_fail(c, e, "event copy");
   gtp_status st = run_window(c, sl.d_net_off, sl.d_ev_t, sl.d_ev_v, ev->net_base ? sl.d_net_base : nullptr,
-                             ev->n_event, ev->t_lo, ev->t_hi);
+                             ev->n_event, ev->t_lo, ev->t_hi, nullptr, ws);
   if (st != GTP_OK) return st;
-  e = cudaEventRecord(sl.free_ev, c->stream);
+  e = cudaEventRecord(sl.free_ev, ws);
+  if (e == cudaSuccess && ws != c->stream) {
+    e = cudaEventRecord(c->walk_done[s_idx], ws);
+    c->walk_pending[s_idx] = true;
+    // work queued on the context's stream from now on follows this walk
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->walk_done[s_idx], 0);
+  }
   if (e != cudaSuccess) return cuda_fail(c, e, "slot order");
   sl.used = true;
   c->next_slot ^= 1;
@@ -756,6 +888,8 @@ gtp_status gtp_push_events_device(gtp_ctx* c, const gtp_events* ev) {
     c->err = "events: missing arrays";
     return GTP_EINVAL;
   }
+  cudaError_t e = join_walks(c, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
   return run_window(c, ev->net_off, ev->time, ev->value_packed, ev->net_base, ev->n_event,
                     ev->t_lo, ev->t_hi);
 }
@@ -779,12 +913,15 @@ gtp_status gtp_push_events_device_ranges(gtp_ctx* c, const gtp_events* ev, const
     c->err = "cycle ranges must lie within the window [t_lo, t_hi)";
     return GTP_EINVAL;
   }
+  cudaError_t e = join_walks(c, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "walk order");
   return run_window(c, ev->net_off, ev->time, ev->value_packed, ev->net_base, ev->n_event, ev->t_lo, ev->t_hi, &r);
 }
 
 gtp_status gtp_sync(gtp_ctx* c) {
   if (!c) return GTP_EINVAL;
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "sync");
   return check_status(c);
 }
@@ -792,7 +929,8 @@ gtp_status gtp_sync(gtp_ctx* c) {
 gtp_status gtp_finalize(gtp_ctx* c) {
   if (!c) return GTP_EINVAL;
   KParams k = make_params(c);
-  cudaError_t e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = launch_finalize(k, c->d_cell_group, c->d_cell5, c->d_cycle5, c->d_tg,
                                   c->d_leak_tmp, c->stream, c->d_cycle5_g, c->d_leak_tmp_g);
   if (e != cudaSuccess) return cuda_fail(c, e, "finalize");
   return GTP_OK;
@@ -802,7 +940,8 @@ void* gtp_get_stream(const gtp_ctx* c) { return c ? static_cast<void*>(c->stream
 
 gtp_status gtp_set_stream(gtp_ctx* c, void* stream) {
   if (!c) return GTP_EINVAL;
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "sync");
   c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
   return GTP_OK;
@@ -871,7 +1010,8 @@ gtp_status gtp_set_cycle_groups(gtp_ctx* c, const int32_t* cell_group, int32_t n
       c->err = "gtp_set_cycle_groups: cell " + std::to_string(i) + " has group out of range";
       return GTP_EINVAL;
     }
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "sync");
   void* old[] = {c->d_cgroup, c->d_cyc_acc_g, c->d_cycle5_g, c->d_leak_tmp_g};
   for (void* q : old)
@@ -945,7 +1085,8 @@ gtp_status gtp_set_cell_range(gtp_ctx* c, int32_t cell_begin, int32_t cell_end) 
       if (P.order_all[i] >= cell_begin && P.order_all[i] < cell_end) order.push_back(P.order_all[i]);
   }
   bb[3] = static_cast<int32_t>(order.size());
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess && !order.empty())
     e = cudaMemcpyAsync(c->d_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -971,6 +1112,8 @@ namespace {
 gtp_status copy_accumulators(gtp_ctx* c, void* dst, const void* src, bool out) {
   if (!c || !dst || !src) return GTP_EINVAL;
   const size_t nc = static_cast<size_t>(c->P.n_cell), ny = static_cast<size_t>(c->P.n_period + 1);
+  cudaError_t ej = join_walks(c, c->stream);
+  if (ej != cudaSuccess) return cuda_fail(c, ej, "walk order");
   struct Seg {
     void* dev;
     size_t bytes;
@@ -1008,7 +1151,9 @@ gtp_status gtp_clock_run_nets(gtp_ctx* c, int32_t* n_clock_nets, int32_t* n_peri
   *n_periodic = 0;
   if (c->n_clk_nets == 0 || !c->d_pclk) return GTP_OK;
   std::vector<int2> tab(static_cast<size_t>(c->P.n_net));
-  cudaError_t e = cudaMemcpyAsync(tab.data(), c->d_pclk, sizeof(int2) * tab.size(), cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(tab.data(), c->d_pclk, sizeof(int2) * tab.size(), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "gtp_clock_run_nets");
   int32_t n = 0;
@@ -1024,8 +1169,9 @@ gtp_status gtp_walk_items(gtp_ctx* c, int64_t* items) {
   const int32_t n_order = c->P.bucket_begin[3];
   if (!c->d_item_off || n_order <= 0 || !c->any_window) return GTP_OK;
   int32_t n = 0;
-  cudaError_t e = cudaMemcpyAsync(&n, c->d_item_off + n_order, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                  c->stream);
+  cudaError_t e = join_walks(c, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&n, c->d_item_off + n_order, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "walk items");
   *items = n;
@@ -1213,6 +1359,9 @@ gtp_status gtp_batch_push_device(gtp_batch* b, const gtp_events* d_ev) {
     gtp_ctx* c = b->ctxs[i];
     if (ev.n_event < 0 || (ev.n_event > 0 && (!ev.time || !ev.value_packed)))
       return batch_fail(b, GTP_EINVAL, "context " + std::to_string(i) + ": malformed events");
+    // the context's host-pushed walks, if any, before its scratch is reused
+    e = join_walks(c, b->stream);
+    if (e != cudaSuccess) return batch_fail(b, GTP_ECUDA, std::string("walk order: ") + cudaGetErrorString(e));
     gtp_status st = prepare_window(c, ev.net_off, ev.time, ev.value_packed, ev.net_base, ev.n_event, ev.t_lo,
                                    ev.t_hi, b->stream, &kwin[i], false);
     if (st != GTP_OK) return batch_fail(b, st, "context " + std::to_string(i) + ": " + c->err);
@@ -1514,6 +1663,9 @@ extern "C" gtp_status gtp_evaluate_noalloc(gtp_ctx* c, const gtp_events* ev, flo
   e = noalloc_scratch(dev, &s);
   if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: cudaGetSymbolAddress");
 
+  // after the context's host-pushed walks, if any (they share its status word)
+  e = join_walks(c, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: walk order");
   // accumulators must start at zero
   e = cudaMemsetAsync(s, 0, off_tg, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "noalloc: clear");

@@ -284,7 +284,13 @@ gtp_status  gtp_reset(gtp_ctx* ctx);
  * per-cell values then cover the evaluated windows only (a spot check of
  * selected cycle ranges, e.g. the learned proxy's audit sample). A window
  * after a gap (or a first window with t_lo > 0) is evaluated on its own: its
- * leakage starts at t_lo from the state its context gives and ends at t_hi. */
+ * leakage starts at t_lo from the state its context gives and ends at t_hi.
+ * Returns once the copy is done (the caller may reuse its buffers); the
+ * walk runs on. Consecutive windows alternate between two device buffers
+ * and two internal streams, so a window's copy overlaps the walk before it
+ * and its walk may start while the last blocks of that walk finish. The
+ * context's stream (gtp_get_stream) waits for each walk: work queued on it
+ * after this returns runs after the window's walk. */
 gtp_status  gtp_push_events(gtp_ctx* ctx, const gtp_events* ev);
 
 /* Same, with events already in device memory (time, value_packed, net_off,
