@@ -1843,10 +1843,12 @@ __global__ void __launch_bounds__(256, WARP_WALK_MIN_BLOCKS) power_warp_kernel(c
 template <int MAXP, bool COUNTS, bool FAST, bool DRIFT, bool RUNS>
 __global__ void __launch_bounds__(256, WALK_MIN_BLOCKS) power_walk_kernel(const __grid_constant__ KParams p) {
   extern __shared__ unsigned long long smem[];
-  if (p.gate_major)
-    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.y, blockIdx.x, gridDim.y, smem);
-  else
-    walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, blockIdx.x, blockIdx.y, gridDim.x, smem);
+  // one call site: the walk's body is inlined once
+  const bool gm = p.gate_major != 0;
+  const int gblk = gm ? blockIdx.y : blockIdx.x;
+  const int tile = gm ? blockIdx.x : blockIdx.y;
+  const int n_blk = gm ? gridDim.y : gridDim.x;
+  walk_block<MAXP, COUNTS, FAST, DRIFT, RUNS, FAST && WALK_USE_RING>(p, gblk, tile, n_blk, smem);
 }
 
 // Persistent walk over the windows of many designs: each block takes work
