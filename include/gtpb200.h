@@ -315,7 +315,9 @@ gtp_status  gtp_push_events_device_ranges(gtp_ctx* ctx, const gtp_events* d_ev, 
 /* Waits for all queued work. */
 gtp_status  gtp_sync(gtp_ctx* ctx);
 
-/* The cudaStream_t (as void*) all of the context's work is queued on.
+/* The cudaStream_t (as void*) the context's work is queued on, or waited
+ * for: the walks of host-pushed windows run on two internal streams, and
+ * this stream waits for each of them (gtp_push_events).
  * gtp_set_stream replaces it with a caller-owned stream (NULL restores the
  * context's own); the caller keeps ownership and must keep it alive. */
 void*       gtp_get_stream(const gtp_ctx* ctx);
