@@ -332,7 +332,9 @@ struct Engine {
     int64_t no_group_match = 0;      // output toggles with a related input but no matching
                                      // `when` group: 0 on the CPU, the default average on CUDA
     int64_t beyond_cuda_cycles = 0;  // toggles in a cycle at or past ceil(time_max / ticks per
-                                     // cycle), which the CUDA kernel never walks
+                                     // cycle): the CUDA kernel's last thread ends one tick past
+                                     // its last cycle, so it walks those at that tick and adds
+                                     // their per-cycle terms past its arrays
     int64_t z_events = 0;            // toggles to or from Z, outside the CUDA 3x3 toggle tables
   };
 
@@ -489,9 +491,9 @@ struct Engine {
         if (!trig[i]) continue;
         const float n_tog = nToggle(prev_st[i], st[i]);
         const bool rise = isRise(prev_st[i], st[i]);
-        // the CUDA kernel walks this event: it toggles, is not the net's first event (the
-        // initial state there) and lies inside its cycles
-        const bool cu_walk = cen && n_tog != 0.0f && frontier[i] - 1 > 0 && cyc < cuda_cycles;
+        // the CUDA kernel walks this event: it toggles and is not the net's first event (the
+        // initial state there)
+        const bool cu_walk = cen && n_tog != 0.0f && frontier[i] - 1 > 0;
         if (cen) {
           ++cen->pin_events;
           if (n_tog != 0.0f) {

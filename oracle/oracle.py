@@ -137,10 +137,12 @@ def divergence_census(design, events, threads: int = 1) -> dict:
     for combinational cells only, near ties); no_group_match - output
     toggles with a related input and no matching `when` group (0 on the
     CPU path, the default average on CUDA); beyond_cuda_cycles - toggles
-    at or past the CUDA kernel's ceil(time_max / ticks per cycle) cycles;
-    z_events - toggles to or from Z. The comparisons cover the events the
-    CUDA kernel walks (toggles after a net's first event, inside its
-    cycles), with one thread over the whole trace."""
+    in a cycle at or past the CUDA kernel's ceil(time_max / ticks per
+    cycle) cycles, whose per-cycle terms it adds past its arrays (its last
+    thread ends one tick after its last cycle); z_events - toggles to or
+    from Z. The comparisons cover the events the CUDA kernel walks
+    (toggles after a net's first event), with one thread over the whole
+    trace."""
     L = lib()
     d = design.c_struct()
     e = events.c_struct()

@@ -104,7 +104,8 @@ def test_output_without_matching_group():
 
 def test_event_past_last_cuda_cycle():
     # time_max 10000 ticks, 1000 ticks a cycle: an event at 10000 is in cycle
-    # 10, which the CUDA kernel does not walk
+    # 10. The CUDA kernel's last thread ends one tick past cycle 10's start,
+    # so it walks the event, and adds its per-cycle terms past its 10 entries
     d = toy.build([toy.inv_cell()], [(0, [0, 1])], 2, time_max=10_000)
     ev = toy.events(2, {0: [(0, 0), (10_000, 1)]})
     expect(census(d, ev), 1, 1, beyond_cuda_cycles=1)
@@ -132,11 +133,12 @@ def test_census_walk_leaves_results_unchanged():
 
 def test_gcd_exposure():
     # the reference's GCD example: 5793 toggles, of which 10 get another
-    # glitch pulse width and 45 lie at the trace's end tick (cycle 26 of 26),
-    # outside the CUDA kernel's cycles; 1211 input lookups at shared ticks
-    # see other states, none with another energy
+    # glitch pulse width and 45 lie at the trace's end tick (t = 125000,
+    # cycle 25: the CPU path's 26th per-cycle entry, one past the CUDA
+    # kernel's 25); 1215 input lookups at shared ticks see other states,
+    # none with another energy
     from gtpower_b200 import tape
     from oracle import oracle as orc
     d, ev, _ = tape.load(os.path.join(HERE, "golden", "gcd_tape.npz"))
     c = orc.divergence_census(d, ev, threads=2)
-    expect(c, 5793, 5793, same_tick_state=1211, glitch_width_diff=10, beyond_cuda_cycles=45)
+    expect(c, 5793, 5793, same_tick_state=1215, glitch_width_diff=10, beyond_cuda_cycles=45)
