@@ -620,6 +620,13 @@ gtp_status gtp_create(const gtp_design* design, const gtp_config* cfg_in, gtp_ct
   if (!c) { set_err("out of host memory"); return GTP_ENOMEM; }
   if (cfg_in) c->cfg = *cfg_in; else gtp_config_default(&c->cfg);
   if (c->cfg.max_n_pin_for_leakage_power <= 0) c->cfg.max_n_pin_for_leakage_power = 16;
+  // the walk kernels are compiled for blocks of at most 256 threads, in warps
+  if (c->cfg.n_thread_per_block != 0 &&
+      (c->cfg.n_thread_per_block < 32 || c->cfg.n_thread_per_block > 256 || c->cfg.n_thread_per_block % 32 != 0)) {
+    set_err("n_thread_per_block must be 0 (256) or a multiple of 32 in [32, 256]");
+    delete c;
+    return GTP_EINVAL;
+  }
   std::string err;
   gtp_status st = pack_design(*design, c->cfg.max_n_pin_for_leakage_power, c->P, err);
   if (st != GTP_OK) { set_err(err); delete c; return st; }

@@ -197,7 +197,7 @@ typedef struct gtp_events {
 typedef struct gtp_config {
   int32_t cuda_device_id;            /* -1 = current device */
   int32_t cycles_per_tile;           /* cycle tile of one CTA; 0 = 768 (512 with cycle groups) */
-  int32_t n_thread_per_block;        /* 0 = auto */
+  int32_t n_thread_per_block;        /* 0 = auto (256); else a multiple of 32 in [32, 256] */
   int32_t gates_per_block;           /* gates one CTA walks per tile; 0 = n_thread_per_block */
   int32_t max_n_pin_for_leakage_power; /* 16 (GlobalConfig.hh:41) */
   int32_t collect_counts;            /* 1 = fill gtp_counts (exact parity) */

@@ -58,11 +58,13 @@ def test_struct_layout_matches_c_compiler(tmp_path):
         assert getattr(_abi.gtp_config, f).offset == int(out[f"gtp_config.{f}"]), f
 
 
-def _create(design):
+def _create(design, **cfg_fields):
     L = _abi.lib()
     d = design.c_struct()
     cfg = _abi.gtp_config()
     L.gtp_config_default(C.byref(cfg))
+    for k, v in cfg_fields.items():
+        setattr(cfg, k, v)
     ctx = C.c_void_p()
     st = L.gtp_create(C.byref(d), C.byref(cfg), C.byref(ctx))
     if st == 0:
@@ -116,6 +118,14 @@ def test_rejects_bad_default_state():
     d.pin_default_state[1] = 3
     st, msg = _create(d)
     assert st == _abi.GTP_EINVAL
+
+
+@pytest.mark.parametrize("threads", [512, 1024, 48, 16, -32])
+def test_rejects_block_size_the_walk_cannot_launch(threads):
+    # the walk kernels are compiled for blocks of at most 256 threads, in
+    # warps; the check comes before any device work
+    st, msg = _create(small(), n_thread_per_block=threads)
+    assert st == _abi.GTP_EINVAL and "n_thread_per_block" in msg
 
 
 def test_pack_values_roundtrip():
