@@ -129,6 +129,16 @@ def workload(args, rank: int):
     return design, info, trace
 
 
+def e2e_cuts(cycles: int, windows: int, ramp: float) -> np.ndarray:
+    """Cycle boundaries [0, c1, ..., cycles] of the e2e windows: `windows`
+    windows whose sizes grow by `ramp` each (a short first copy; each later
+    copy hides behind the walk of the window before), rounded to whole
+    cycles, empty windows dropped."""
+    sizes = ramp ** np.arange(windows)
+    cuts = np.concatenate([[0], np.round(np.cumsum(sizes) / sizes.sum() * cycles)]).astype(np.int64)
+    return np.unique(cuts)
+
+
 def algorithmic_bytes(design, n_event: int) -> int:
     """8 B tick + 2 bits per net event, CSR offsets, 24 B of attributes per
     pin, the LUT floats, and 20 B of outputs per cell and per cycle."""
@@ -791,9 +801,7 @@ def main():
         if args.e2e_split == "ramp":
             from gtpower_b200 import windows as _windows
             tpc = design.ticks_per_cycle
-            sizes = args.e2e_ramp ** np.arange(args.e2e_windows)
-            cuts = np.concatenate([[0], np.round(np.cumsum(sizes) / sizes.sum() * args.cycles)]).astype(np.int64)
-            cuts = np.unique(cuts)
+            cuts = e2e_cuts(args.cycles, args.e2e_windows, args.e2e_ramp)
             wins_src = [_windows.make_window(ev, tpc, int(cuts[k]) * tpc,
                                              int(cuts[k + 1]) * tpc if k + 2 < len(cuts) else np.iinfo(np.int64).max)
                         for k in range(len(cuts) - 1)]
