@@ -117,9 +117,12 @@ def read_spef_caps(path: str) -> dict[str, float]:
 
 def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock_port: str,
                  period: float, input_slew: float, timescale: float, time_max: int,
-                 voltage: float) -> tuple[Design, dict]:
+                 voltage: float, ideal_clock_slew: float | None = None) -> tuple[Design, dict]:
     """Design for the instances whose cell has Liberty data (others are
-    black boxes the power walk skips, as the reference does)."""
+    black boxes the power walk skips, as the reference does).
+    ideal_clock_slew: the slew of every clock-network net when the clock is
+    ideal (OpenSTA's clock transition, set_clock_transition, 0 by default);
+    None propagates the clock buffers' slews like any other net."""
     insts = [i for i in mod.instances if i.cell in cells]
     used = sorted({i.cell for i in insts})
     lib = CellLibrary([cells[c] for c in used])
@@ -170,12 +173,35 @@ def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock
         driver[pin_net[q]] = q
     pin_cell = np.repeat(np.arange(len(insts)), np.diff(pin_off))
 
-    # slews in topological order over combinational arcs
+    # clock network: nets reached from the clock port through combinational cells
+    clock_nets = {nets[clock_port]} if clock_port in nets else set()
+    changed = True
+    while changed:
+        changed = False
+        for k, inst in enumerate(insts):
+            c = cells[inst.cell]
+            if c["is_sequential"]:
+                continue
+            ins = [pin_net[pin_off[k] + j] for j in range(c["n_in"])]
+            outs = [pin_net[pin_off[k] + j] for j in range(c["n_in"], len(c["pins"]))]
+            if any(m in clock_nets for m in ins):
+                for m in outs:
+                    if m >= 0 and m not in clock_nets:
+                        clock_nets.add(m)
+                        changed = True
+    # slews in topological order over combinational arcs; with an ideal clock
+    # (no propagated clock in the SDC) every clock-network net takes the
+    # clock's ideal transition, as OpenSTA gives an ideal clock's pins
     net_slew = np.full((2, n_net), np.nan)
     for p in mod.inputs:
         net_slew[:, nets[p]] = input_slew
+    if ideal_clock_slew is not None:
+        for m in clock_nets:
+            net_slew[:, m] = ideal_clock_slew
     resolved = ~np.isnan(net_slew[0])
     pending = set(np.nonzero(driver >= 0)[0].tolist())
+    if ideal_clock_slew is not None:
+        pending -= clock_nets
     for _ in range(len(insts) + 2):
         progressed = False
         for n in list(pending):
@@ -236,22 +262,6 @@ def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock
                 dl = _interp2(tab, np.asarray([float(s)]), np.asarray([float(pin_load[pin_off[k] + n_in + o])]))[0]
                 arc[arc_off[k] + (o * n_in + qq) * 4 + 2 * fr + to] = np.float32(dl)
 
-    # clock network: nets reached from the clock port through combinational cells
-    clock_nets = {nets[clock_port]} if clock_port in nets else set()
-    changed = True
-    while changed:
-        changed = False
-        for k, inst in enumerate(insts):
-            c = cells[inst.cell]
-            if c["is_sequential"]:
-                continue
-            ins = [pin_net[pin_off[k] + j] for j in range(c["n_in"])]
-            outs = [pin_net[pin_off[k] + j] for j in range(c["n_in"], len(c["pins"]))]
-            if any(m in clock_nets for m in ins):
-                for m in outs:
-                    if m >= 0 and m not in clock_nets:
-                        clock_nets.add(m)
-                        changed = True
     group = np.zeros(len(insts), np.uint8)
     for k, inst in enumerate(insts):
         c = cells[inst.cell]

@@ -37,7 +37,7 @@ def build(ref_root: str):
     cells = {c: lib.cell_data(c) for c in used}
     d, info = netlist.build_design(mod, cells, caps, clock_port="clk", period=5e-9,
                                    input_slew=0.1e-9, timescale=v.timescale,
-                                   time_max=v.time_max, voltage=lib.voltage)
+                                   time_max=v.time_max, voltage=lib.voltage, ideal_clock_slew=0.0)
     # bind waveforms: design nets, then instance pins (VCD order, later wins)
     nets = info["nets"]
     pin_index = {n: k for k, n in enumerate(info["pin_names"])}
