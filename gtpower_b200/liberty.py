@@ -418,10 +418,16 @@ class Library:
         for p in ordered:
             pname = p.args[0].strip('"')
             capv = p.attr("capacitance")
+            cap = float(capv) * self.cap_scale if capv is not None else 0.0
+            # rise_capacitance / fall_capacitance override it per edge
+            # (LibertyReader::visitRiseCap, visitFallCap)
+            rcap, fcap = p.attr("rise_capacitance"), p.attr("fall_capacitance")
             out["pins"].append({
                 "name": pname,
                 "direction": p.attr("direction", "").strip('"'),
-                "capacitance": float(capv) * self.cap_scale if capv is not None else 0.0,
+                "capacitance": cap,
+                "rise_capacitance": float(rcap) * self.cap_scale if rcap is not None else cap,
+                "fall_capacitance": float(fcap) * self.cap_scale if fcap is not None else cap,
                 "clock": str(p.attr("clock", "false")).strip('"') == "true",
             })
             fn = p.attr("function")

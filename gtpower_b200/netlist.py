@@ -5,8 +5,9 @@ connections), lumped net capacitance from SPEF (*D_NET totals), and builds
 a `Design` with the per-pin quantities an STA run would provide:
 
   - load cap of an output pin = SPEF total cap of its net + the Liberty
-    capacitance of the net's load pins (GraphDelayCalc::loadCap with lumped
-    parasitics);
+    capacitance of the net's load pins, for the rise and the fall edge
+    (rise_capacitance / fall_capacitance where the library gives them),
+    the larger of the two (GraphDelayCalc::loadCap with lumped parasitics);
   - slews: primary inputs take the SDC input transition; each driver
     output takes the worst rise_transition / fall_transition of its delay
     arcs at (worst input slew, load cap), propagated in topological order;
@@ -153,21 +154,27 @@ def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock
 
     # driver of each net and load caps
     is_out = np.zeros(n_pin, bool)
-    pin_cap = np.zeros(n_pin)
+    pin_cap = np.zeros((2, n_pin))        # rise, fall
     pin_clock_attr = np.zeros(n_pin, np.uint8)
     for k, inst in enumerate(insts):
         c = cells[inst.cell]
         for j, p in enumerate(c["pins"]):
             q = pin_off[k] + j
             is_out[q] = j >= c["n_in"]
-            pin_cap[q] = p["capacitance"]
+            pin_cap[0, q] = p.get("rise_capacitance", p["capacitance"])
+            pin_cap[1, q] = p.get("fall_capacitance", p["capacitance"])
             pin_clock_attr[q] = 1 if p["clock"] else 0
     net_cap = np.zeros(n_net)
     for name, n in nets.items():
         net_cap[n] = spef_caps.get(name, 0.0)
-    load = net_cap.copy()
+    # the larger of the rise and fall loads (wire + the load pins' caps of
+    # that edge), as GraphDelayCalc::loadCap takes over both edges
     valid = pin_net >= 0
-    np.add.at(load, pin_net[valid & ~is_out], pin_cap[valid & ~is_out])
+    ld = valid & ~is_out
+    load_rf = np.stack([net_cap.copy(), net_cap.copy()])
+    for e in range(2):
+        np.add.at(load_rf[e], pin_net[ld], pin_cap[e, ld])
+    load = np.maximum(load_rf[0], load_rf[1])
     driver = np.full(n_net, -1, np.int64)
     for q in np.nonzero(valid & is_out)[0]:
         driver[pin_net[q]] = q

@@ -71,8 +71,8 @@ def test_oracle_against_reference_report(group):
     ok_int, ok_sw, ok_leak, ok_tot = POWER_VCD_OK[group]
     assert leakage == pytest.approx(ok_leak, rel=0.015)         # state-only: within 1.5%
     assert internal == pytest.approx(ok_int, rel=0.01)          # slew-dependent: within 1%
-    assert switching == pytest.approx(ok_sw, rel=0.08)          # load-cap-dependent: within 8%
-    assert internal + switching + leakage == pytest.approx(ok_tot, rel=0.03)
+    assert switching == pytest.approx(ok_sw, rel=0.05)          # load-cap-dependent: within 5%
+    assert internal + switching + leakage == pytest.approx(ok_tot, rel=0.015)
 
 
 def test_report_power_table_layout(tmp_path):
