@@ -118,12 +118,17 @@ def read_spef_caps(path: str) -> dict[str, float]:
 
 def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock_port: str,
                  period: float, input_slew: float, timescale: float, time_max: int,
-                 voltage: float, ideal_clock_slew: float | None = None) -> tuple[Design, dict]:
+                 voltage: float, ideal_clock_slew: float | None = None,
+                 input_slews: dict[str, float] | None = None,
+                 port_loads: dict[str, float] | None = None) -> tuple[Design, dict]:
     """Design for the instances whose cell has Liberty data (others are
     black boxes the power walk skips, as the reference does).
     ideal_clock_slew: the slew of every clock-network net when the clock is
     ideal (OpenSTA's clock transition, set_clock_transition, 0 by default);
-    None propagates the clock buffers' slews like any other net."""
+    None propagates the clock buffers' slews like any other net.
+    input_slews: per-port slews (s) that replace input_slew for those ports;
+    port_loads: external load (F) on top-level ports (SDC set_load), added
+    to the load of the port's net."""
     insts = [i for i in mod.instances if i.cell in cells]
     used = sorted({i.cell for i in insts})
     lib = CellLibrary([cells[c] for c in used])
@@ -174,6 +179,9 @@ def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock
     load_rf = np.stack([net_cap.copy(), net_cap.copy()])
     for e in range(2):
         np.add.at(load_rf[e], pin_net[ld], pin_cap[e, ld])
+    for port, c_ext in (port_loads or {}).items():
+        if port in nets:
+            load_rf[:, nets[port]] += c_ext
     load = np.maximum(load_rf[0], load_rf[1])
     driver = np.full(n_net, -1, np.int64)
     for q in np.nonzero(valid & is_out)[0]:
@@ -201,7 +209,7 @@ def build_design(mod: Module, cells: dict, spef_caps: dict[str, float], *, clock
     # clock's ideal transition, as OpenSTA gives an ideal clock's pins
     net_slew = np.full((2, n_net), np.nan)
     for p in mod.inputs:
-        net_slew[:, nets[p]] = input_slew
+        net_slew[:, nets[p]] = (input_slews or {}).get(p, input_slew)
     if ideal_clock_slew is not None:
         for m in clock_nets:
             net_slew[:, m] = ideal_clock_slew

@@ -8,7 +8,11 @@ the transitions come from the SDC:
 
   - create_clock -period P [-name N] [-waveform {...}] PORT: the clock port
     and period;
-  - set_input_transition T PORTS: the slew of primary inputs;
+  - set_input_transition T PORTS: the slew of primary inputs (all of them
+    for [all_inputs], else the ports named, glob patterns allowed; later
+    commands win);
+  - set_load C PORTS: external load on top-level ports, added to their
+    nets' load (in the library's capacitance unit);
   - set_clock_transition T CLOCKS: the ideal clock's transition (0 when
     unset), which every pin of an ideal clock's network takes;
   - set_propagated_clock: clock-network slews are propagated through the
@@ -32,9 +36,10 @@ from __future__ import annotations
 
 import argparse
 import ast
+import fnmatch
 import operator
 import re
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -46,9 +51,13 @@ from .design import Design, Events
 class Sdc:
     clock_port: str | None = None
     period: float | None = None          # s
-    input_transition: float = 0.0        # s
+    input_transition: float = 0.0        # s, for [all_inputs]
     clock_transition: float = 0.0        # s
     propagated: bool = False
+    # (port pattern, value) in command order: transitions in s, loads in
+    # library capacitance units
+    port_transitions: list = field(default_factory=list)
+    port_loads: list = field(default_factory=list)
 
 
 _BINOPS = {ast.Add: operator.add, ast.Sub: operator.sub, ast.Mult: operator.mul,
@@ -168,7 +177,17 @@ def read_sdc(text: str, time_unit: float) -> Sdc:
         elif cmd == "set_input_transition":
             vals = [a for a in args if not a.startswith("-")]
             if vals:
-                sdc.input_transition = float(vals[0]) * time_unit
+                v = float(vals[0]) * time_unit
+                ports = " ".join(vals[1:]).split()
+                if not ports or "__all_inputs__" in ports:
+                    sdc.input_transition = v
+                    sdc.port_transitions = []        # all inputs: earlier per-port values are replaced
+                else:
+                    sdc.port_transitions += [(pt, v) for pt in ports]
+        elif cmd == "set_load":
+            vals = [a for a in args if not a.startswith("-")]
+            if len(vals) >= 2:
+                sdc.port_loads += [(pt, float(vals[0])) for pt in " ".join(vals[1:]).split()]
         elif cmd == "set_clock_transition":
             vals = [a for a in args if not a.startswith("-")]
             if vals:
@@ -192,10 +211,23 @@ def build_tape(lib_path: str, verilog_path: str, spef_path: str | None, sdc_path
         raise ValueError("the SDC defines no clock (create_clock -period ... PORT)")
     used = sorted({i.cell for i in mod.instances if i.cell in lib.cells})
     cells = {c: lib.cell_data(c) for c in used}
+    input_slews = {}
+    for pat, val in sdc.port_transitions:
+        for port in mod.inputs:
+            if fnmatch.fnmatchcase(port, pat):
+                input_slews[port] = val
+    port_loads: dict[str, float] = {}
+    for pat, val in sdc.port_loads:
+        ports = mod.outputs if pat == "__all_outputs__" else (
+            mod.inputs if pat == "__all_inputs__" else
+            [p for p in mod.inputs + mod.outputs if fnmatch.fnmatchcase(p, pat)])
+        for port in ports:
+            port_loads[port] = val * lib.cap_scale
     d, info = netlist.build_design(mod, cells, caps, clock_port=sdc.clock_port, period=sdc.period,
                                    input_slew=sdc.input_transition, timescale=v.timescale,
                                    time_max=v.time_max, voltage=lib.voltage,
-                                   ideal_clock_slew=None if sdc.propagated else sdc.clock_transition)
+                                   ideal_clock_slew=None if sdc.propagated else sdc.clock_transition,
+                                   input_slews=input_slews, port_loads=port_loads)
     # bind waveforms: design nets, then instance pins (VCD order, later wins)
     nets = info["nets"]
     pin_index = {n: k for k, n in enumerate(info["pin_names"])}

@@ -135,7 +135,12 @@ def _vcd():
     return "\n".join(rows) + "\n"
 
 
+def _args(f):
+    return f["lib"], f["v"], f["spef"], f["sdc"], f["vcd"], "tb/dut"
+
+
 def _files(tmp_path, sdc=SDC):
+    tmp_path.mkdir(parents=True, exist_ok=True)
     paths = {}
     for name, text in (("lib", LIB), ("v", VERILOG), ("spef", SPEF), ("sdc", sdc), ("vcd", _vcd())):
         p = tmp_path / f"top.{name}"
@@ -163,6 +168,29 @@ def test_sdc_subset():
     assert s.clock_transition == pytest.approx(0.03e-9)
     assert not s.propagated
     assert read_sdc(text + "\nset_propagated_clock [all_clocks]\n", 1e-9).propagated
+
+
+def test_sdc_port_transitions_and_loads():
+    from gtpower_b200.sta_tape import read_sdc
+    s = read_sdc("set_input_transition 0.3 [get_ports {a b*}]\n"
+                 "set_input_transition 0.1 [all_inputs]\n"
+                 "set_input_transition 0.4 [get_ports a]\n"
+                 "set_load 0.02 [all_outputs]\n", 1e-9)
+    assert s.input_transition == pytest.approx(0.1e-9)
+    assert s.port_transitions == [("a", pytest.approx(0.4e-9))]   # the [all_inputs] line replaced 0.3
+    assert s.port_loads == [("__all_outputs__", 0.02)]
+
+
+def test_tape_honours_port_transition_and_load(tmp_path):
+    from gtpower_b200 import sta_tape
+    base, _, _ = sta_tape.build_tape(*_args(_files(tmp_path / "a")))
+    f = _files(tmp_path / "b", SDC + "set_input_transition 0.5 [get_ports a]\nset_load 0.03 [get_ports y]\n")
+    d, _, _ = sta_tape.build_tape(*_args(f))
+    k = {n: i for i, n in enumerate(d.cell_names)}
+    u1_a = d.cell_pin_off[k["u1"]]
+    u2_y = d.cell_pin_off[k["u2"]] + 1
+    assert d.pin_slew_rise[u1_a] == pytest.approx(0.5e-9)
+    assert d.pin_load_cap[u2_y] == pytest.approx(base.pin_load_cap[u2_y] + 0.03e-12, rel=1e-6)
 
 
 def test_sdc_rejects_code():
