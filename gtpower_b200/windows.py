@@ -58,3 +58,34 @@ def split(events: Events, tpc: int, cycle_edges: list[int]) -> list[Events]:
         t_hi = cycle_edges[k + 1] * tpc if k + 2 < len(cycle_edges) else np.iinfo(np.int64).max
         out.append(make_window(events, tpc, t_lo, t_hi))
     return out
+
+
+def interval_edges(events: Events, tpc: int, max_events: int) -> list[int]:
+    """Cycle edges [0, c1, ..., cn] of time intervals holding about
+    max_events listed events each, by the reference's rule: the events are
+    counted in time order, and when the count since the last cut passes
+    max_events the interval ends at the time of the event that passed it,
+    whose events then start nothing (power/VcdReader.cc:292-296); interval
+    bounds are rounded up to cycle boundaries and empty intervals dropped
+    (power/cuda/CudaPower.cu:1263-1272). The last edge is the cycle after
+    the last event."""
+    if max_events <= 0:
+        raise ValueError("max_events must be positive")
+    t = np.sort(np.asarray(events.time, dtype=np.int64))
+    edges = [0]
+    i = max_events                       # the (max_events + 1)-th event from the interval start
+    while i < t.shape[0]:
+        c = -(-int(t[i]) // tpc)         # ceil to a cycle boundary
+        if c > edges[-1]:
+            edges.append(c)
+        i += max_events + 1
+    last = (int(t[-1]) // tpc + 1) if t.shape[0] else 1
+    if last > edges[-1]:
+        edges.append(last)
+    return edges
+
+
+def split_by_events(events: Events, tpc: int, max_events: int) -> list[Events]:
+    """The trace as windows with context over interval_edges(events, tpc,
+    max_events); the last window runs past the trace."""
+    return split(events, tpc, interval_edges(events, tpc, max_events))
