@@ -481,6 +481,11 @@ class Library:
 
 
 def read_library(path: str) -> Library:
+    """A Liberty file, plain or gzip-compressed (.gz)."""
+    if path.endswith(".gz"):
+        import gzip
+        with gzip.open(path, "rt") as f:
+            return Library(parse(f.read()))
     with open(path) as f:
         return Library(parse(f.read()))
 

@@ -245,6 +245,19 @@ def test_propagated_clock_takes_buffer_slews(tmp_path):
     assert d.pin_slew_rise[clk_pin] > 0.01e-9       # the buffer's rise_transition at its load
 
 
+def test_gzipped_library(tmp_path):
+    import gzip
+    from gtpower_b200 import liberty
+    p = tmp_path / "tiny.lib.gz"
+    with gzip.open(p, "wt") as f:
+        f.write(LIB)
+    lib = liberty.read_library(str(p))
+    assert sorted(lib.cells) == ["CLKBUFX", "DFFX", "INVX"]
+    pins = lib.cell_data("INVX")["pins"]
+    assert pins[0]["rise_capacitance"] == pytest.approx(0.0024e-12)
+    assert pins[0]["fall_capacitance"] == pytest.approx(0.0018e-12)
+
+
 def test_command_line(tmp_path):
     from gtpower_b200 import sta_tape, tape
     f = _files(tmp_path)
