@@ -5,7 +5,6 @@ the gcd_tb VCD, scope gcd_tb/gcd1, as test/gcd/power_vcd.tcl reads them).
 Runs only where the reference tree is present; it writes
   tests/golden/gcd_tape.npz     design + events (the engine's inputs)
   tests/golden/gcd_oracle.npz   FP64 oracle outputs on that tape
-  tests/golden/gcd_report.txt   report_power table from the oracle totals
 
 The tape comes from gtpower_b200.sta_tape: slews, load caps and arc delays
 from gtpower_b200.netlist's STA approximation, the clock and transitions
